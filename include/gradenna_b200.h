@@ -1,0 +1,154 @@
+/*
+ * gradenna_b200 -- C ABI of the B200 (sm_100a) FDTD time-stepping library.
+ *
+ * This header is the drop-in boundary that replaces the reference's native
+ * FFI for the FDTD hot path:
+ *
+ *   reference symbol                              replaced by
+ *   ------------------------------------------------------------------------
+ *   gradenna_tm_run_f32 / _f64                    gdn_tm_run_f32 / _f64
+ *     (rust/src/lib.rs:89-142, bound in src/gradenna/native.py:140-170)
+ *   gradenna_3d_run_f32 / _f64                    gdn_3d_run_f32 / _f64
+ *     (rust/src/lib3d.rs:191-230, bound in src/gradenna/native3d.py:145-163)
+ *   simulate_tm_native / simulate_3d_native       the Python shim
+ *     (src/gradenna/native.py:200, native3d.py:174) gradenna_b200.simulate_tm
+ *
+ * Conventions (all entry points):
+ *   - Every entry point returns a GdnStatus (0 = success) and never aborts;
+ *     gdn_last_error() gives a one-line message for the calling thread.
+ *     (The reference Rust kernels return void and abort on panic.)
+ *   - Bulk arrays (coefficient tables, waveforms, outputs, workspace) are
+ *     DEVICE pointers on the current CUDA device. The small index lists in the
+ *     *Points structs are HOST pointers (they are binned by tile on the host).
+ *   - Arrays are C-order (last axis contiguous) with the reference's shapes:
+ *     ez (nx, ny), hx (nx, ny-1), hy (nx-1, ny); waveforms (n_steps, n).
+ *   - Complex DFT outputs are interleaved (re, im) pairs, float (complex64)
+ *     or double (complex128) as selected by dft_f64, shape (n_freq, ...).
+ *     Output DFT buffers are written, not accumulated into: the library zeroes
+ *     them. (The reference required caller-zeroed outputs: native.py:409-423.)
+ *   - Work is enqueued on `stream` (a cudaStream_t; NULL = legacy default)
+ *     and the call returns without synchronising, except where a status must
+ *     be read back (documented per entry point).
+ *   - The caller owns every buffer. Scratch: pass `workspace` of at least
+ *     gdn_*_workspace_size() bytes, or NULL to let the library allocate it
+ *     stream-ordered for the duration of the call.
+ */
+#ifndef GRADENNA_B200_H
+#define GRADENNA_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum GdnStatus {
+  GDN_OK = 0,
+  GDN_ERR_BAD_ARG = 1,     /* invalid sizes, indices or null pointers         */
+  GDN_ERR_OOM = 2,         /* device allocation failed                          */
+  GDN_ERR_CUDA = 3,        /* a CUDA runtime call failed                        */
+  GDN_ERR_TIMEOUT = 4,     /* a bounded device-side wait gave up                */
+  GDN_ERR_NONFINITE = 5,   /* a NaN/Inf was detected where it is checked       */
+  GDN_ERR_UNSUPPORTED = 6  /* requested feature not built for this device       */
+} GdnStatus;
+
+/* Library version string, e.g. "gradenna_b200 0.1 (sm_100a)". */
+const char* gdn_version(void);
+
+/* Message describing the last non-zero status returned on this thread. */
+const char* gdn_last_error(void);
+
+/* ------------------------------------------------------------------------ */
+/* 2D TM                                                                    */
+/* ------------------------------------------------------------------------ */
+
+/* Scalar description of one 2D TM run. Mirrors the reference SimParams
+ * (rust/src/lib.rs:56-69, native.py:124-137) plus the scalars the Rust entry
+ * point took by value (lib.rs:123-129). */
+typedef struct GdnTmParams {
+  int32_t nx, ny;          /* Ez grid, >= 3 each and > 2*npml + 2            */
+  int32_t npml;            /* CPML thickness (cells per side), 0 = PEC box    */
+  int32_t n_steps;         /* time steps                                      */
+  int32_t n_sources;       /* Jz line sources (Ez cells)                      */
+  int32_t n_ports;         /* lumped RVS ports (Ez cells)                     */
+  int32_t n_mx, n_my;      /* magnetic-current sources on the Hx / Hy grids   */
+  int32_t n_probes;        /* Ez probes                                       */
+  int32_t n_freq;          /* running-DFT frequencies (0 = no DFT)            */
+  int32_t record_energy;   /* 1: write the total field energy every step      */
+  int32_t dft_f64;         /* 1: complex128 accumulators, 0: complex64        */
+  int32_t cw_sources;      /* 1: Jz/Mx/My waveforms synthesised on the device
+                              from per-source CW phasor weights (see buffers) */
+  int32_t use_dft_region;  /* 0: full-grid DFT; 1: per-component rectangles   */
+  /* Per-component DFT rectangles [lo, hi) in each component's own index
+   * space, order ez, hx, hy; used when use_dft_region = 1. An empty
+   * rectangle (hi <= lo on either axis) means "not accumulated". */
+  int32_t dft_lo[3][2];
+  int32_t dft_hi[3][2];
+  double dt, dx, dy, dz;   /* dz = unit length of the 2D slice (DZ = 1 m)     */
+  double mu0;              /* vacuum permeability used by the energy record   */
+} GdnTmParams;
+
+/* Host-memory point lists (int32 pairs split into i and j arrays). */
+typedef struct GdnTmPoints {
+  const int32_t *src_i, *src_j;     /* n_sources, margin 1                    */
+  const int32_t *port_i, *port_j;   /* n_ports, margin 1                      */
+  const int32_t *mx_i, *mx_j;       /* n_mx, on the Hx grid (nx, ny-1)        */
+  const int32_t *my_i, *my_j;       /* n_my, on the Hy grid (nx-1, ny)        */
+  const int32_t *probe_i, *probe_j; /* n_probes, margin 0                     */
+} GdnTmPoints;
+
+/* Device buffers. Field-typed arrays are float for *_f32, double for *_f64.
+ * Argument-for-argument this is the reference's pointer list
+ * (native.py:152-170 / lib.rs:96-142), grouped. */
+typedef struct GdnTmBuffers {
+  const void *ca, *cb, *eps;               /* (nx, ny); eps only if energy    */
+  const void *inv_kx_e, *inv_ky_e;         /* (nx-2), (ny-2)                  */
+  const void *inv_kx_h, *inv_ky_h;         /* (nx-1), (ny-1)                  */
+  /* CPML slab b/c tables, each of length npml: ezx, ezy, hyx, hxy x lo/hi */
+  const void *b_ezx_lo, *c_ezx_lo, *b_ezx_hi, *c_ezx_hi;
+  const void *b_ezy_lo, *c_ezy_lo, *b_ezy_hi, *c_ezy_hi;
+  const void *b_hyx_lo, *c_hyx_lo, *b_hyx_hi, *c_hyx_hi;
+  const void *b_hxy_lo, *c_hxy_lo, *b_hxy_hi, *c_hxy_hi;
+  double dt_mu, inv_dx, inv_dy;            /* scalars, cast to the field type */
+  const void *cb_src;                      /* (n_sources)                     */
+  const void *src_cur;                     /* (n_steps, n_sources)            */
+  const void *cb_vs;                       /* (n_ports)                       */
+  const void *port_vs;                     /* (n_steps, n_ports)              */
+  const void *mx_cur, *my_cur;             /* (n_steps, n_mx), (n_steps, n_my)*/
+  /* CW-source mode (cw_sources = 1): waveforms are
+   *   J_m(n) = env[n] * sum_k Re(W[m,k] * exp(+i w_k t_n))
+   * with t_n = (n+1) dt for Jz and (n+1/2) dt for Mx/My; W is complex128
+   * (n_src, n_freq); exp(+i w t) is the conjugate of ph_e / ph_h. In this
+   * mode src_cur / mx_cur / my_cur are ignored. */
+  const double *cw_env;                    /* (n_steps)                       */
+  const double *src_w, *mx_w, *my_w;       /* complex128 (n, n_freq)          */
+  /* Exact-phase tables exp(-2 pi i f t_n), complex128 (n_steps, n_freq):
+   * t_n = (n+1) dt for ph_e, (n+1/2) dt for ph_h (fdtd2d.py:393-398). */
+  const double *ph_e, *ph_h;
+  /* outputs */
+  void *ez, *hx, *hy;                      /* final fields                    */
+  void *out_probe;                         /* (n_steps, n_probes)             */
+  void *out_v, *out_i;                     /* (n_steps, n_ports)              */
+  void *out_energy;                        /* (n_steps)                       */
+  void *dft_ez, *dft_hx, *dft_hy;          /* (n_freq, region shape), x dt    */
+  void *workspace;                         /* NULL: allocated by the library  */
+  size_t workspace_bytes;
+} GdnTmBuffers;
+
+/* Scratch bytes needed by gdn_tm_run_* for these parameters. */
+int gdn_tm_workspace_size(const GdnTmParams* p, int f64, size_t* bytes);
+
+/* Run the whole 2D TM time loop (replaces gradenna_tm_run_f32/_f64,
+ * rust/src/lib.rs:89-641). Stream-ordered; host index lists are consumed
+ * before return. */
+int gdn_tm_run_f32(const GdnTmParams* p, const GdnTmPoints* pts,
+                   const GdnTmBuffers* b, void* stream);
+int gdn_tm_run_f64(const GdnTmParams* p, const GdnTmPoints* pts,
+                   const GdnTmBuffers* b, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* GRADENNA_B200_H */
