@@ -39,11 +39,14 @@ class TmParams(ctypes.Structure):
         ("nx", c_int32), ("ny", c_int32), ("npml", c_int32), ("n_steps", c_int32),
         ("n_sources", c_int32), ("n_ports", c_int32), ("n_mx", c_int32), ("n_my", c_int32),
         ("n_probes", c_int32), ("n_freq", c_int32), ("record_energy", c_int32),
-        ("dft_f64", c_int32), ("cw_sources", c_int32), ("use_dft_region", c_int32),
-        ("dft_lo", (c_int32 * 2) * 3), ("dft_hi", (c_int32 * 2) * 3),
+        ("dft_f64", c_int32), ("cw_sources", c_int32), ("n_monitors", c_int32),
         ("dt", c_double), ("dx", c_double), ("dy", c_double), ("dz", c_double),
         ("mu0", c_double),
     ]
+
+
+class DftMonitor(ctypes.Structure):
+    _fields_ = [("comp", c_int32), ("lo", c_int32 * 3), ("hi", c_int32 * 3), ("out", c_void_p)]
 
 
 class TmPoints(ctypes.Structure):
@@ -53,6 +56,7 @@ class TmPoints(ctypes.Structure):
         ("mx_i", P_i32), ("mx_j", P_i32),
         ("my_i", P_i32), ("my_j", P_i32),
         ("probe_i", P_i32), ("probe_j", P_i32),
+        ("monitors", ctypes.POINTER(DftMonitor)),
     ]
 
 

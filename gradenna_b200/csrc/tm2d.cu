@@ -10,16 +10,25 @@
 //   injection and V record (:446-451) -> running DFT (:453-458) -> probes.
 //
 // B200 design:
-//   * Field state lives in a RING of R slots (ez, hx, hy per slot, rows padded
-//     to `ld`). Step n reads slot n%R and writes slot (n+1)%R, so every slot
-//     is a snapshot of the fields after one step. The H and E kernels of a
-//     step therefore never update in place, and the running DFT is folded
-//     into the accumulators once per T = R-1 steps by one kernel that reads
-//     T snapshots: accumulator read-modify-write traffic drops by T.
-//   * Point work (sources, ports, probes, magnetic currents) is binned by
-//     tile on the host; the CTA owning a tile applies it after its sweep, so
-//     no extra launches are needed per step.
-//   * One chunk of T steps (2T sweeps + DFT fold + step-counter advance) is
+//   * One fused kernel per time step. A CTA owns a TI x TJ tile of Ez cells;
+//     it stages Ez^n, Hx, Hy for the tile plus a one-cell halo in shared
+//     memory with 16-byte cp.async copies, recomputes the halo row/column of
+//     H^{n+1/2} that its E update needs (instead of a second launch and a
+//     grid-wide dependency), updates E, applies the tile's point work
+//     (sources, ports, probes, magnetic currents) in shared memory and writes
+//     the tile back with 16-byte stores.
+//   * Field state lives in a RING of R slots (ez, hx, hy planes per slot).
+//     Step n reads slot n%R and writes slot (n+1)%R, so halo reads never race
+//     with the owner's writes, and every slot is a snapshot of the fields
+//     after one step. The running DFT is folded into the accumulators once
+//     per T = R-1 steps by one kernel that reads the T snapshots, so the
+//     accumulator read-modify-write traffic drops by T.
+//   * Planes are padded (one ghost row above/below, PADJ ghost columns on
+//     each side, rows a multiple of the tile) so every halo copy is aligned
+//     and in bounds; ghost cells stay zero, which is also the PEC ring.
+//   * H-type psi (updated redundantly on halo cells) is double-buffered by
+//     step parity; E-type psi is updated only by its owner, in place.
+//   * One chunk of T steps (T step kernels + DFT fold + counter advance) is
 //     captured once as a CUDA graph and replayed; kernels read the absolute
 //     step index from a device counter.
 #include <algorithm>
@@ -30,26 +39,35 @@
 namespace gdn {
 namespace tm2d {
 
-constexpr int TJ = 32;  // tile width (contiguous axis)
-constexpr int TI = 8;   // tile height
+constexpr int TI = 16;    // tile rows (x, slow axis)
+constexpr int TJ = 64;    // tile columns (y, contiguous axis)
+constexpr int HALO = 4;   // column halo in shared memory (16 B of f32)
+constexpr int PADJ = 32;  // ghost columns on each side of a plane
+constexpr int NT = 256;   // threads per CTA
+constexpr int EW = TJ + 2 * HALO;
 constexpr int KMAX = 16;
+
+struct Pt {
+  int m, i, j, pad;  // point index, cell (i, j)
+};
 
 template <typename T>
 struct Dev {
-  int nx, ny, ld, npml, R, n_steps, n_freq, tiles_x;
-  long long slot;  // elements per ring slot (3 * nx * ld)
+  int nx, ny, ld, npml, R, n_steps, n_freq;
+  long long plane, slot;  // elements per plane and per ring slot (3 planes)
   T* ring;
-  const T *ca, *cb, *eps;
+  const T *ca, *cb, *eps;  // ca/cb: padded planes; eps: caller (nx, ny)
   const T *ikx_e, *iky_e, *ikx_h, *iky_h;
   const T *b_ezx_lo, *c_ezx_lo, *b_ezx_hi, *c_ezx_hi;
   const T *b_ezy_lo, *c_ezy_lo, *b_ezy_hi, *c_ezy_hi;
   const T *b_hyx_lo, *c_hyx_lo, *b_hyx_hi, *c_hyx_hi;
   const T *b_hxy_lo, *c_hxy_lo, *b_hxy_hi, *c_hxy_hi;
-  T *ezx_lo, *ezx_hi, *ezy_lo, *ezy_hi, *hyx_lo, *hyx_hi, *hxy_lo, *hxy_hi;
+  T *ezx_lo, *ezx_hi, *ezy_lo, *ezy_hi;
+  T *hyx_lo[2], *hyx_hi[2], *hxy_lo[2], *hxy_hi[2];
   T dt_mu, inv_dx, inv_dy, dx, dy, dz;
   int n_src, n_ports, n_mx, n_my, n_probes;
   const int *src_off, *port_off, *mx_off, *my_off, *probe_off;
-  const int2 *src_pts, *port_pts, *mx_pts, *my_pts, *probe_pts;
+  const Pt *src_pts, *port_pts, *mx_pts, *my_pts, *probe_pts;
   const T *cb_src, *src_cur, *cb_vs, *port_vs, *mx_cur, *my_cur;
   int cw;
   const double* cw_env;
@@ -58,11 +76,25 @@ struct Dev {
   const int* step_base;
 };
 
-template <typename A>
-struct DftDev {
-  int lo[3][2], hi[3][2];
-  typename Cplx<A>::type* acc[3];
+// Device copy of one DFT monitor (GdnDftMonitor resolved against the grid).
+struct Mon {
+  int comp, lo0, lo1, w;
+  long long count;
+  void* out;
 };
+
+// Offset of field cell (i, j) in a padded plane.
+__device__ __forceinline__ long long cell_at(int ld, int i, int j) {
+  return (long long)(i + 1) * ld + (j + PADJ);
+}
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+  const unsigned s = static_cast<unsigned>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
 
 // Value of a point source waveform at step n: tabulated, or synthesised from
 // CW phasor weights, J(n) = env[n] Re(sum_k W_k conj(ph[n,k])).
@@ -72,170 +104,213 @@ __device__ __forceinline__ T point_value(const Dev<T>& d, const T* cur, const do
   if (!d.cw) return cur[(long long)n * n_pts + m];
   double s = 0.0;
   for (int k = 0; k < d.n_freq; ++k) {
-    double2 a = w[(long long)m * d.n_freq + k];
-    double2 p = ph[(long long)n * d.n_freq + k];
+    const double2 a = w[(long long)m * d.n_freq + k];
+    const double2 p = ph[(long long)n * d.n_freq + k];
     s += a.x * p.x + a.y * p.y;
   }
   return T(d.cw_env[n] * s);
 }
 
+// One CPML psi recursion (cpml.py:120-158): psi' = b psi + c diff, returns
+// diff/kappa + psi'. `store` is false on halo cells owned by another CTA.
 template <typename T>
-__device__ __forceinline__ void atomic_add(T* p, T v) {
-  atomicAdd(p, v);
+__device__ __forceinline__ T psi_term(T diff, T ikappa, T b, T c, const T* src, T* dst,
+                                      bool store) {
+  const T p = b * *src + c * diff;
+  if (store) *dst = p;
+  return diff * ikappa + p;
 }
 
 // ---------------------------------------------------------------------------
-// H sweep: E^n -> H^{n+1/2}  (fdtd2d.py:416-428; lib.rs:298-375)
+// Fused step: E^n -> H^{n+1/2} -> E^{n+1} on one tile, plus point work.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(TI * TJ) tm_h_sweep(Dev<T> d, int sub) {
+__global__ void __launch_bounds__(NT) tm_step(Dev<T> d, int sub) {
+  __shared__ __align__(16) T sEz[TI + 2][EW];  // rows i0-1..i0+TI, cols j0-HALO..
+  __shared__ __align__(16) T sHx[TI][EW];      // rows i0..i0+TI-1, cols j0-HALO..
+  __shared__ __align__(16) T sHy[TI + 1][TJ];  // rows i0-1..i0+TI-1, cols j0..
+  __shared__ __align__(16) T sE1[TI][TJ];      // new Ez of the tile
+
   const int n = *d.step_base + sub;
+  const int par = n & 1;
   const int nx = d.nx, ny = d.ny, ld = d.ld, npml = d.npml;
+  const int i0 = blockIdx.y * TI, j0 = blockIdx.x * TJ;
+  const int tid = threadIdx.x;
   const T* ez0 = d.ring + (long long)(n % d.R) * d.slot;
-  const T* hx0 = ez0 + (long long)nx * ld;
-  const T* hy0 = hx0 + (long long)nx * ld;
-  T* hx1 = d.ring + (long long)((n + 1) % d.R) * d.slot + (long long)nx * ld;
-  T* hy1 = hx1 + (long long)nx * ld;
-
-  const int j = blockIdx.x * TJ + threadIdx.x;
-  const int i = blockIdx.y * TI + threadIdx.y;
-  const long long c = (long long)i * ld + j;
-  if (i < nx && j < ny - 1) {
-    const T diff = (ez0[c + 1] - ez0[c]) * d.inv_dy;
-    T term = diff;
-    if (j < npml) {
-      T* ps = d.hxy_lo + (long long)i * npml + j;
-      const T p = d.b_hxy_lo[j] * *ps + d.c_hxy_lo[j] * diff;
-      *ps = p;
-      term = diff * d.iky_h[j] + p;
-    } else if (j >= ny - 1 - npml) {
-      const int s = j - (ny - 1 - npml);
-      T* ps = d.hxy_hi + (long long)i * npml + s;
-      const T p = d.b_hxy_hi[s] * *ps + d.c_hxy_hi[s] * diff;
-      *ps = p;
-      term = diff * d.iky_h[j] + p;
-    }
-    hx1[c] = hx0[c] - d.dt_mu * term;
-  }
-  if (i < nx - 1 && j < ny) {
-    const T diff = (ez0[c + ld] - ez0[c]) * d.inv_dx;
-    T term = diff;
-    if (i < npml) {
-      T* ps = d.hyx_lo + (long long)i * ny + j;
-      const T p = d.b_hyx_lo[i] * *ps + d.c_hyx_lo[i] * diff;
-      *ps = p;
-      term = diff * d.ikx_h[i] + p;
-    } else if (i >= nx - 1 - npml) {
-      const int s = i - (nx - 1 - npml);
-      T* ps = d.hyx_hi + (long long)s * ny + j;
-      const T p = d.b_hyx_hi[s] * *ps + d.c_hyx_hi[s] * diff;
-      *ps = p;
-      term = diff * d.ikx_h[i] + p;
-    }
-    hy1[c] = hy0[c] + d.dt_mu * term;
-  }
-
-  // Magnetic-current injection on this tile: H -= (dt/mu) M (fdtd2d.py:419-428).
-  const int tile = blockIdx.y * gridDim.x + blockIdx.x;
-  const int mb = d.mx_off[tile], me = d.mx_off[tile + 1];
-  const int yb = d.my_off[tile], ye = d.my_off[tile + 1];
-  if (mb < me || yb < ye) {
-    __syncthreads();
-    const int tid = threadIdx.y * TJ + threadIdx.x;
-    for (int q = mb + tid; q < me; q += TI * TJ) {
-      const int2 pt = d.mx_pts[q];
-      atomic_add(hx1 + pt.y, -(d.dt_mu * point_value(d, d.mx_cur, d.mx_w, d.ph_h, d.n_mx, pt.x, n)));
-    }
-    for (int q = yb + tid; q < ye; q += TI * TJ) {
-      const int2 pt = d.my_pts[q];
-      atomic_add(hy1 + pt.y, -(d.dt_mu * point_value(d, d.my_cur, d.my_w, d.ph_h, d.n_my, pt.x, n)));
-    }
-  }
-}
-
-// ---------------------------------------------------------------------------
-// E sweep: H^{n+1/2} -> E^{n+1} on the interior, then Jz / ports / probes
-// (fdtd2d.py:430-461; lib.rs:389-535)
-// ---------------------------------------------------------------------------
-template <typename T>
-__global__ void __launch_bounds__(TI * TJ) tm_e_sweep(Dev<T> d, int sub) {
-  const int n = *d.step_base + sub;
-  const int nx = d.nx, ny = d.ny, ld = d.ld, npml = d.npml;
-  const T* ez0 = d.ring + (long long)(n % d.R) * d.slot;
+  const T* hx0 = ez0 + d.plane;
+  const T* hy0 = hx0 + d.plane;
   T* ez1 = d.ring + (long long)((n + 1) % d.R) * d.slot;
-  const T* hx1 = ez1 + (long long)nx * ld;
-  const T* hy1 = hx1 + (long long)nx * ld;
+  T* hx1 = ez1 + d.plane;
+  T* hy1 = hx1 + d.plane;
 
-  const int j = blockIdx.x * TJ + threadIdx.x;
-  const int i = blockIdx.y * TI + threadIdx.y;
-  const long long c = (long long)i * ld + j;
-  if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2) {
-    const T dhy_dx = (hy1[c] - hy1[c - ld]) * d.inv_dx;
-    const T dhx_dy = (hx1[c] - hx1[c - 1]) * d.inv_dy;
-    T tx = dhy_dx, ty = dhx_dy;
-    const int a = i - 1, b = j - 1;
-    const int nxi = nx - 2, nyi = ny - 2;
-    if (a < npml) {
-      T* ps = d.ezx_lo + (long long)a * nyi + b;
-      const T p = d.b_ezx_lo[a] * *ps + d.c_ezx_lo[a] * dhy_dx;
-      *ps = p;
-      tx = dhy_dx * d.ikx_e[a] + p;
-    } else if (a >= nxi - npml) {
-      const int s = a - (nxi - npml);
-      T* ps = d.ezx_hi + (long long)s * nyi + b;
-      const T p = d.b_ezx_hi[s] * *ps + d.c_ezx_hi[s] * dhy_dx;
-      *ps = p;
-      tx = dhy_dx * d.ikx_e[a] + p;
+  // ---- stage the tile + halo (16-byte async copies) ----
+  constexpr int V = 16 / sizeof(T);
+  for (int q = tid; q < (TI + 2) * (EW / V); q += NT) {
+    const int r = q / (EW / V), c = (q - r * (EW / V)) * V;
+    cp_async16(&sEz[r][c], ez0 + cell_at(ld, i0 - 1 + r, j0 - HALO + c));
+  }
+  for (int q = tid; q < TI * (EW / V); q += NT) {
+    const int r = q / (EW / V), c = (q - r * (EW / V)) * V;
+    cp_async16(&sHx[r][c], hx0 + cell_at(ld, i0 + r, j0 - HALO + c));
+  }
+  for (int q = tid; q < (TI + 1) * (TJ / V); q += NT) {
+    const int r = q / (TJ / V), c = (q - r * (TJ / V)) * V;
+    cp_async16(&sHy[r][c], hy0 + cell_at(ld, i0 - 1 + r, j0 + c));
+  }
+  cp_async_wait_all();
+  __syncthreads();
+
+  // ---- H sweep (fdtd2d.py:416-428) on the tile + its halo row/column ----
+  const T* hxy_lo_r = d.hxy_lo[par];
+  const T* hxy_hi_r = d.hxy_hi[par];
+  T* hxy_lo_w = d.hxy_lo[par ^ 1];
+  T* hxy_hi_w = d.hxy_hi[par ^ 1];
+  for (int q = tid; q < TI * (TJ + 1); q += NT) {
+    const int r = q / (TJ + 1), cc = q - r * (TJ + 1) - 1;  // cc = -1 is the halo column
+    const int i = i0 + r, j = j0 + cc;
+    if (i < nx && j >= 0 && j < ny - 1) {
+      const T diff = (sEz[r + 1][HALO + cc + 1] - sEz[r + 1][HALO + cc]) * d.inv_dy;
+      T term = diff;
+      if (j < npml) {
+        const long long o = (long long)i * npml + j;
+        term = psi_term(diff, d.iky_h[j], d.b_hxy_lo[j], d.c_hxy_lo[j], hxy_lo_r + o,
+                        hxy_lo_w + o, cc >= 0);
+      } else if (j >= ny - 1 - npml) {
+        const int s = j - (ny - 1 - npml);
+        const long long o = (long long)i * npml + s;
+        term = psi_term(diff, d.iky_h[j], d.b_hxy_hi[s], d.c_hxy_hi[s], hxy_hi_r + o,
+                        hxy_hi_w + o, cc >= 0);
+      }
+      sHx[r][HALO + cc] -= d.dt_mu * term;
     }
-    if (b < npml) {
-      T* ps = d.ezy_lo + (long long)a * npml + b;
-      const T p = d.b_ezy_lo[b] * *ps + d.c_ezy_lo[b] * dhx_dy;
-      *ps = p;
-      ty = dhx_dy * d.iky_e[b] + p;
-    } else if (b >= nyi - npml) {
-      const int s = b - (nyi - npml);
-      T* ps = d.ezy_hi + (long long)a * npml + s;
-      const T p = d.b_ezy_hi[s] * *ps + d.c_ezy_hi[s] * dhx_dy;
-      *ps = p;
-      ty = dhx_dy * d.iky_e[b] + p;
+  }
+  const T* hyx_lo_r = d.hyx_lo[par];
+  const T* hyx_hi_r = d.hyx_hi[par];
+  T* hyx_lo_w = d.hyx_lo[par ^ 1];
+  T* hyx_hi_w = d.hyx_hi[par ^ 1];
+  for (int q = tid; q < (TI + 1) * TJ; q += NT) {
+    const int r = q / TJ, c = q - r * TJ;  // r = 0 is the halo row i0-1
+    const int i = i0 - 1 + r, j = j0 + c;
+    if (i >= 0 && i < nx - 1 && j < ny) {
+      const T diff = (sEz[r + 1][HALO + c] - sEz[r][HALO + c]) * d.inv_dx;
+      T term = diff;
+      if (i < npml) {
+        const long long o = (long long)i * ny + j;
+        term = psi_term(diff, d.ikx_h[i], d.b_hyx_lo[i], d.c_hyx_lo[i], hyx_lo_r + o,
+                        hyx_lo_w + o, r > 0);
+      } else if (i >= nx - 1 - npml) {
+        const int s = i - (nx - 1 - npml);
+        const long long o = (long long)s * ny + j;
+        term = psi_term(diff, d.ikx_h[i], d.b_hyx_hi[s], d.c_hyx_hi[s], hyx_hi_r + o,
+                        hyx_hi_w + o, r > 0);
+      }
+      sHy[r][c] += d.dt_mu * term;
     }
-    const long long g = (long long)i * ny + j;
-    ez1[c] = d.ca[g] * ez0[c] + d.cb[g] * (tx - ty);
+  }
+  __syncthreads();
+
+  // Magnetic currents on the tile and its halo: H -= (dt/mu) M (fdtd2d.py:419-428).
+  const int tile = blockIdx.y * gridDim.x + blockIdx.x;
+  {
+    const int mb = d.mx_off[tile], me = d.mx_off[tile + 1];
+    const int yb = d.my_off[tile], ye = d.my_off[tile + 1];
+    if (mb < me || yb < ye) {
+      for (int q = mb + tid; q < me; q += NT) {
+        const Pt pt = d.mx_pts[q];
+        atomicAdd(&sHx[pt.i - i0][HALO + pt.j - j0],
+                  -(d.dt_mu * point_value(d, d.mx_cur, d.mx_w, d.ph_h, d.n_mx, pt.m, n)));
+      }
+      for (int q = yb + tid; q < ye; q += NT) {
+        const Pt pt = d.my_pts[q];
+        atomicAdd(&sHy[pt.i - (i0 - 1)][pt.j - j0],
+                  -(d.dt_mu * point_value(d, d.my_cur, d.my_w, d.ph_h, d.n_my, pt.m, n)));
+      }
+      __syncthreads();
+    }
   }
 
-  const int tile = blockIdx.y * gridDim.x + blockIdx.x;
+  // Owned H^{n+1/2} back to the ring (ghost cells carry their zeros).
+  for (int q = tid; q < TI * (TJ / V); q += NT) {
+    const int r = q / (TJ / V), c = (q - r * (TJ / V)) * V;
+    *reinterpret_cast<uint4*>(hx1 + cell_at(ld, i0 + r, j0 + c)) =
+        *reinterpret_cast<const uint4*>(&sHx[r][HALO + c]);
+    *reinterpret_cast<uint4*>(hy1 + cell_at(ld, i0 + r, j0 + c)) =
+        *reinterpret_cast<const uint4*>(&sHy[r + 1][c]);
+  }
+
+  // ---- E sweep on the interior (fdtd2d.py:438-443) ----
+  const int nxi = nx - 2, nyi = ny - 2;
+  for (int q = tid; q < TI * TJ; q += NT) {
+    const int r = q / TJ, c = q - r * TJ;
+    const int i = i0 + r, j = j0 + c;
+    T e1 = sEz[r + 1][HALO + c];
+    if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2) {
+      const T dhy_dx = (sHy[r + 1][c] - sHy[r][c]) * d.inv_dx;
+      const T dhx_dy = (sHx[r][HALO + c] - sHx[r][HALO + c - 1]) * d.inv_dy;
+      T tx = dhy_dx, ty = dhx_dy;
+      const int a = i - 1, b = j - 1;
+      if (a < npml) {
+        T* ps = d.ezx_lo + (long long)a * nyi + b;
+        tx = psi_term(dhy_dx, d.ikx_e[a], d.b_ezx_lo[a], d.c_ezx_lo[a], ps, ps, true);
+      } else if (a >= nxi - npml) {
+        const int s = a - (nxi - npml);
+        T* ps = d.ezx_hi + (long long)s * nyi + b;
+        tx = psi_term(dhy_dx, d.ikx_e[a], d.b_ezx_hi[s], d.c_ezx_hi[s], ps, ps, true);
+      }
+      if (b < npml) {
+        T* ps = d.ezy_lo + (long long)a * npml + b;
+        ty = psi_term(dhx_dy, d.iky_e[b], d.b_ezy_lo[b], d.c_ezy_lo[b], ps, ps, true);
+      } else if (b >= nyi - npml) {
+        const int s = b - (nyi - npml);
+        T* ps = d.ezy_hi + (long long)a * npml + s;
+        ty = psi_term(dhx_dy, d.iky_e[b], d.b_ezy_hi[s], d.c_ezy_hi[s], ps, ps, true);
+      }
+      const long long g = cell_at(ld, i, j);
+      e1 = d.ca[g] * e1 + d.cb[g] * (tx - ty);
+    }
+    sE1[r][c] = e1;
+  }
+
+  // ---- point work on the new Ez (fdtd2d.py:430-461) ----
   const int sb = d.src_off[tile], se = d.src_off[tile + 1];
   const int pb = d.port_off[tile], pe = d.port_off[tile + 1];
   const int qb = d.probe_off[tile], qe = d.probe_off[tile + 1];
   if (sb < se || pb < pe || qb < qe) {
-    const int tid = threadIdx.y * TJ + threadIdx.x;
     __syncthreads();
-    // Jz line sources: Ez -= cb_src * J (fdtd2d.py:444).
-    for (int q = sb + tid; q < se; q += TI * TJ) {
-      const int2 pt = d.src_pts[q];
-      atomic_add(ez1 + pt.y, -(d.cb_src[pt.x] * point_value(d, d.src_cur, d.src_w, d.ph_e, d.n_src, pt.x, n)));
+    // Jz line sources: Ez -= cb_src J (fdtd2d.py:444).
+    for (int q = sb + tid; q < se; q += NT) {
+      const Pt pt = d.src_pts[q];
+      atomicAdd(&sE1[pt.i - i0][pt.j - j0],
+                -(d.cb_src[pt.m] * point_value(d, d.src_cur, d.src_w, d.ph_e, d.n_src, pt.m, n)));
     }
     __syncthreads();
-    // RVS ports, in port order (fdtd2d.py:430-436, 446-451): all injections
-    // on this tile first, then the V/I records.
+    // RVS ports in port order: every injection first, then the V/I records.
     if (tid == 0 && pb < pe) {
       for (int q = pb; q < pe; ++q) {
-        const int2 pt = d.port_pts[q];
-        ez1[pt.y] += -(d.cb_vs[pt.x] * d.port_vs[(long long)n * d.n_ports + pt.x]);
+        const Pt pt = d.port_pts[q];
+        sE1[pt.i - i0][pt.j - j0] += -(d.cb_vs[pt.m] * d.port_vs[(long long)n * d.n_ports + pt.m]);
       }
       for (int q = pb; q < pe; ++q) {
-        const int2 pt = d.port_pts[q];
-        const long long p = pt.y;
-        const T cur = (hy1[p] - hy1[p - ld]) * d.dy - (hx1[p] - hx1[p - 1]) * d.dx;
-        d.out_i[(long long)n * d.n_ports + pt.x] = cur;
-        d.out_v[(long long)n * d.n_ports + pt.x] = T(-0.5) * d.dz * (ez0[p] + ez1[p]);
+        const Pt pt = d.port_pts[q];
+        const int r = pt.i - i0, c = pt.j - j0;
+        const T cur = (sHy[r + 1][c] - sHy[r][c]) * d.dy -
+                      (sHx[r][HALO + c] - sHx[r][HALO + c - 1]) * d.dx;
+        d.out_i[(long long)n * d.n_ports + pt.m] = cur;
+        d.out_v[(long long)n * d.n_ports + pt.m] =
+            T(-0.5) * d.dz * (sEz[r + 1][HALO + c] + sE1[r][c]);
       }
     }
     __syncthreads();
-    for (int q = qb + tid; q < qe; q += TI * TJ) {
-      const int2 pt = d.probe_pts[q];
-      d.out_probe[(long long)n * d.n_probes + pt.x] = ez1[pt.y];
+    for (int q = qb + tid; q < qe; q += NT) {
+      const Pt pt = d.probe_pts[q];
+      d.out_probe[(long long)n * d.n_probes + pt.m] = sE1[pt.i - i0][pt.j - j0];
     }
+  }
+  __syncthreads();
+  for (int q = tid; q < TI * (TJ / V); q += NT) {
+    const int r = q / (TJ / V), c = (q - r * (TJ / V)) * V;
+    *reinterpret_cast<uint4*>(ez1 + cell_at(ld, i0 + r, j0 + c)) =
+        *reinterpret_cast<const uint4*>(&sE1[r][c]);
   }
 }
 
@@ -244,9 +319,10 @@ __global__ void __launch_bounds__(TI * TJ) tm_e_sweep(Dev<T> d, int sub) {
 // accumulated cell, acc_k += sum_t ph[n0+t, k] * x_t, partial sums in A.
 // ---------------------------------------------------------------------------
 template <typename T, typename A>
-__global__ void __launch_bounds__(256) tm_dft_fold(Dev<T> d, DftDev<A> q, int sub0, int cnt) {
+__global__ void __launch_bounds__(256) tm_dft_fold(Dev<T> d, const Mon* mons, int sub0, int cnt) {
   extern __shared__ unsigned char smem_raw[];
   A* sph = reinterpret_cast<A*>(smem_raw);  // [2 tables][cnt][K][re, im]
+  using C = typename Cplx<A>::type;
   const int n0 = *d.step_base + sub0;
   const int K = d.n_freq;
   for (int idx = threadIdx.x; idx < cnt * K; idx += blockDim.x) {
@@ -259,17 +335,13 @@ __global__ void __launch_bounds__(256) tm_dft_fold(Dev<T> d, DftDev<A> q, int su
     sph[2 * (cnt * K + idx) + 1] = A(ph.y);
   }
   __syncthreads();
-  const int comp = blockIdx.y;
-  const int h = q.hi[comp][0] - q.lo[comp][0];
-  const int w = q.hi[comp][1] - q.lo[comp][1];
-  if (h <= 0 || w <= 0) return;
-  const long long count = (long long)h * w;
+  const Mon mon = mons[blockIdx.y];
   const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= count) return;
-  const int ri = int(r / w), rj = int(r - (long long)ri * w);
-  const int i = q.lo[comp][0] + ri, j = q.lo[comp][1] + rj;
-  const A* ph = sph + (comp == 0 ? 0 : 2 * cnt * K);
-  const long long field_off = (long long)comp * d.nx * d.ld + (long long)i * d.ld + j;
+  if (r >= mon.count) return;
+  const int ri = int(r / mon.w), rj = int(r - (long long)ri * mon.w);
+  const A* ph = sph + (mon.comp == 0 ? 0 : 2 * cnt * K);
+  const long long field_off =
+      (long long)mon.comp * d.plane + cell_at(d.ld, mon.lo0 + ri, mon.lo1 + rj);
   A are[KMAX], aim[KMAX];
 #pragma unroll
   for (int k = 0; k < KMAX; ++k) are[k] = aim[k] = A(0);
@@ -285,14 +357,14 @@ __global__ void __launch_bounds__(256) tm_dft_fold(Dev<T> d, DftDev<A> q, int su
       }
     }
   }
-  typename Cplx<A>::type* acc = q.acc[comp] + r;
+  C* acc = static_cast<C*>(mon.out) + r;
 #pragma unroll
   for (int k = 0; k < KMAX; ++k) {
     if (k < K) {
-      typename Cplx<A>::type v = acc[(long long)k * count];
+      C v = acc[(long long)k * mon.count];
       v.x += are[k];
       v.y += aim[k];
-      acc[(long long)k * count] = v;
+      acc[(long long)k * mon.count] = v;
     }
   }
 }
@@ -303,18 +375,18 @@ template <typename T>
 __global__ void tm_energy(Dev<T> d, double* eacc, int sub) {
   const int n = *d.step_base + sub;
   const T* ez1 = d.ring + (long long)((n + 1) % d.R) * d.slot;
-  const T* hx1 = ez1 + (long long)d.nx * d.ld;
-  const T* hy1 = hx1 + (long long)d.nx * d.ld;
+  const T* hx1 = ez1 + d.plane;
+  const T* hy1 = hx1 + d.plane;
   double ue = 0.0, uh = 0.0;
   const long long total = (long long)d.nx * d.ny;
   for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
        g += (long long)gridDim.x * blockDim.x) {
     const int i = int(g / d.ny), j = int(g - (long long)i * d.ny);
-    const long long c = (long long)i * d.ld + j;
+    const long long c = cell_at(d.ld, i, j);
     const double e = double(ez1[c]);
     ue += double(d.eps[g]) * e * e;
-    if (j < d.ny - 1) uh += double(hx1[c]) * double(hx1[c]);
-    if (i < d.nx - 1) uh += double(hy1[c]) * double(hy1[c]);
+    const double hx = double(hx1[c]), hy = double(hy1[c]);  // zero outside their grids
+    uh += hx * hx + hy * hy;
   }
   for (int o = 16; o > 0; o >>= 1) {
     ue += __shfl_down_sync(0xffffffffu, ue, o);
@@ -344,24 +416,36 @@ __global__ void tm_energy(Dev<T> d, double* eacc, int sub) {
 
 template <typename T>
 __global__ void tm_energy_finish(const double* eacc, T* out, int n_steps, double cell,
-                                     double mu0) {
+                                 double mu0) {
   const int n = blockIdx.x * blockDim.x + threadIdx.x;
   if (n < n_steps) out[n] = T(0.5 * eacc[2 * n] * cell + 0.5 * mu0 * eacc[2 * n + 1] * cell);
 }
 
 __global__ void tm_advance(int* step_base, int cnt) { *step_base += cnt; }
 
-// Copy the final ring slot into the caller's unpadded ez/hx/hy.
+// Copy a caller (nx, ny) array into a padded plane (ca, cb at set-up).
 template <typename T>
-__global__ void tm_copy_out(const T* slot, int nx, int ny, int ld, T* ez, T* hx, T* hy) {
+__global__ void tm_pad_in(const T* src, T* dst, int nx, int ny, int ld) {
   const long long total = (long long)nx * ny;
   for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
        g += (long long)gridDim.x * blockDim.x) {
     const int i = int(g / ny), j = int(g - (long long)i * ny);
-    const long long c = (long long)i * ld + j;
+    dst[cell_at(ld, i, j)] = src[g];
+  }
+}
+
+// Copy the final ring slot into the caller's unpadded ez/hx/hy.
+template <typename T>
+__global__ void tm_copy_out(const T* slot, long long plane, int nx, int ny, int ld, T* ez, T* hx,
+                            T* hy) {
+  const long long total = (long long)nx * ny;
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
+       g += (long long)gridDim.x * blockDim.x) {
+    const int i = int(g / ny), j = int(g - (long long)i * ny);
+    const long long c = cell_at(ld, i, j);
     ez[g] = slot[c];
-    if (j < ny - 1) hx[(long long)i * (ny - 1) + j] = slot[(long long)nx * ld + c];
-    if (i < nx - 1) hy[g] = slot[2LL * nx * ld + c];
+    if (j < ny - 1) hx[(long long)i * (ny - 1) + j] = slot[plane + c];
+    if (i < nx - 1) hy[g] = slot[2 * plane + c];
   }
 }
 
@@ -380,10 +464,11 @@ __global__ void tm_dft_scale(C* a, long long count, double s) {
 // Host side
 // ---------------------------------------------------------------------------
 
+
 struct Layout {
-  int ld = 0, R = 2, T = 32, tiles_x = 0, tiles_y = 0, n_tiles = 0;
-  long long slot = 0;
-  size_t ring, psi[8], off[5], pts[5], step, eacc, total;
+  int ld = 0, rows = 0, R = 2, T = 32, tiles_x = 0, tiles_y = 0, n_tiles = 0;
+  long long plane = 0, slot = 0;
+  size_t ring, ca, cb, psi_e[4], psi_h[8], psi_end, off[5], pts[5], mons, step, eacc, total;
 };
 
 static int dft_block_steps(const GdnTmParams* p, size_t slot_bytes) {
@@ -396,29 +481,72 @@ static int dft_block_steps(const GdnTmParams* p, size_t slot_bytes) {
 
 static Layout make_layout(const GdnTmParams* p, size_t esize) {
   Layout L;
-  L.ld = int(div_up(p->ny, 32) * 32);
-  L.slot = 3LL * p->nx * L.ld;
-  L.T = dft_block_steps(p, size_t(L.slot) * esize);
-  L.R = p->n_freq > 0 ? L.T + 1 : 2;
-  L.tiles_x = L.ld / TJ;
+  L.tiles_x = int(div_up(p->ny, TJ));
   L.tiles_y = int(div_up(p->nx, TI));
   L.n_tiles = L.tiles_x * L.tiles_y;
+  L.ld = PADJ + L.tiles_x * TJ + PADJ;
+  L.rows = L.tiles_y * TI + 2;
+  L.plane = (long long)L.rows * L.ld;
+  L.slot = 3 * L.plane;
+  L.T = dft_block_steps(p, size_t(L.slot) * esize);
+  L.R = p->n_freq > 0 ? L.T + 1 : 2;
   Carve cv;
   L.ring = cv.take<char>(size_t(L.R) * L.slot * esize);
-  const int m = p->npml, nx = p->nx, ny = p->ny;
-  const size_t psz[8] = {size_t(m) * (ny - 2), size_t(m) * (ny - 2), size_t(nx - 2) * m,
-                         size_t(nx - 2) * m,   size_t(m) * ny,       size_t(m) * ny,
-                         size_t(nx) * m,       size_t(nx) * m};
-  for (int k = 0; k < 8; ++k) L.psi[k] = cv.take<char>(psz[k] * esize);
+  L.ca = cv.take<char>(size_t(L.plane) * esize);
+  L.cb = cv.take<char>(size_t(L.plane) * esize);
+  const size_t m = size_t(p->npml), nx = size_t(p->nx), ny = size_t(p->ny);
+  const size_t pe[4] = {m * (ny - 2), m * (ny - 2), (nx - 2) * m, (nx - 2) * m};
+  for (int k = 0; k < 4; ++k) L.psi_e[k] = cv.take<char>(std::max<size_t>(pe[k], 1) * esize);
+  const size_t ph[4] = {m * ny, m * ny, nx * m, nx * m};  // hyx lo/hi, hxy lo/hi
+  for (int k = 0; k < 8; ++k) L.psi_h[k] = cv.take<char>(std::max<size_t>(ph[k / 2], 1) * esize);
+  L.psi_end = cv.take<char>(0);
   const int counts[5] = {p->n_sources, p->n_ports, p->n_mx, p->n_my, p->n_probes};
   for (int k = 0; k < 5; ++k) {
     L.off[k] = cv.take<int>(L.n_tiles + 1);
-    L.pts[k] = cv.take<int2>(std::max(counts[k], 1));
+    L.pts[k] = cv.take<Pt>(2 * size_t(std::max(counts[k], 1)));
   }
+  L.mons = cv.take<Mon>(size_t(std::max(p->n_monitors, 3)));
   L.step = cv.take<int>(1);
   L.eacc = cv.take<double>(p->record_energy ? 2 * size_t(std::max(p->n_steps, 1)) : 1);
   L.total = cv.bytes();
   return L;
+}
+
+// Bin point records by the tiles that need them. kind 0: the owner tile of
+// an Ez cell; kind 1: Hx cells, also the right neighbour whose halo column
+// holds them; kind 2: Hy cells, also the lower neighbour whose halo row
+// holds them.
+struct Bins {
+  std::vector<int> off;
+  std::vector<Pt> pts;
+};
+
+static Bins bin_tiles(int n, const int32_t* pi, const int32_t* pj, const Layout& L, int kind) {
+  std::vector<std::pair<int, Pt>> rec;
+  rec.reserve(2 * size_t(n));
+  for (int m = 0; m < n; ++m) {
+    const int i = pi[m], j = pj[m];
+    const int tx = j / TJ, ty = i / TI;
+    Pt pt{m, i, j, 0};
+    rec.push_back({ty * L.tiles_x + tx, pt});
+    if (kind == 1 && (j + 1) % TJ == 0 && tx + 1 < L.tiles_x)
+      rec.push_back({ty * L.tiles_x + tx + 1, pt});
+    if (kind == 2 && (i + 1) % TI == 0 && ty + 1 < L.tiles_y)
+      rec.push_back({(ty + 1) * L.tiles_x + tx, pt});
+  }
+  std::stable_sort(rec.begin(), rec.end(),
+                   [](const std::pair<int, Pt>& a, const std::pair<int, Pt>& b) {
+                     return a.first < b.first;
+                   });
+  Bins b;
+  b.off.assign(L.n_tiles + 1, 0);
+  b.pts.resize(rec.size());
+  for (size_t k = 0; k < rec.size(); ++k) {
+    b.off[rec[k].first + 1]++;
+    b.pts[k] = rec[k].second;
+  }
+  for (int t = 0; t < L.n_tiles; ++t) b.off[t + 1] += b.off[t];
+  return b;
 }
 
 static int validate(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuffers* b) {
@@ -478,32 +606,30 @@ static int validate(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuf
       GDN_BAD_ARG("source waveform arrays are null");
   }
   if (p->n_sources && !b->cb_src) GDN_BAD_ARG("cb_src is null");
-  if (p->n_freq > 0) {
-    if (!b->dft_ez || !b->dft_hx || !b->dft_hy) {
-      if (!p->use_dft_region) GDN_BAD_ARG("dft output buffers are null");
-    }
-    if (p->use_dft_region) {
-      const int shp[3][2] = {{nx, ny}, {nx, ny - 1}, {nx - 1, ny}};
-      void* const outs[3] = {b->dft_ez, b->dft_hx, b->dft_hy};
-      for (int c = 0; c < 3; ++c) {
-        const int* lo = p->dft_lo[c];
-        const int* hi = p->dft_hi[c];
-        if (hi[0] <= lo[0] || hi[1] <= lo[1]) continue;
-        if (lo[0] < 0 || lo[1] < 0 || hi[0] > shp[c][0] || hi[1] > shp[c][1])
-          GDN_BAD_ARG("dft region %d [%d,%d)x[%d,%d) outside its component", c, lo[0], hi[0],
-                      lo[1], hi[1]);
-        if (!outs[c]) GDN_BAD_ARG("dft output %d is null", c);
-      }
+  if (p->n_monitors < 0) GDN_BAD_ARG("n_monitors must be >= 0");
+  if (p->n_freq > 0 && p->n_monitors == 0 && (!b->dft_ez || !b->dft_hx || !b->dft_hy))
+    GDN_BAD_ARG("dft output buffers are null");
+  if (p->n_freq > 0 && p->n_monitors > 0) {
+    if (!pts->monitors) GDN_BAD_ARG("monitor list is null");
+    const int shp[3][2] = {{nx, ny}, {nx, ny - 1}, {nx - 1, ny}};
+    for (int k = 0; k < p->n_monitors; ++k) {
+      const GdnDftMonitor& m = pts->monitors[k];
+      if (m.comp < 0 || m.comp > 2) GDN_BAD_ARG("monitor %d: component %d not in 0..2", k, m.comp);
+      if (m.lo[0] < 0 || m.lo[1] < 0 || m.hi[0] > shp[m.comp][0] || m.hi[1] > shp[m.comp][1] ||
+          m.hi[0] <= m.lo[0] || m.hi[1] <= m.lo[1])
+        GDN_BAD_ARG("monitor %d: box [%d,%d)x[%d,%d) empty or outside component %d", k, m.lo[0],
+                    m.hi[0], m.lo[1], m.hi[1], m.comp);
+      if (!m.out) GDN_BAD_ARG("monitor %d: output is null", k);
     }
   }
   if (p->dt <= 0 || p->dx <= 0 || p->dy <= 0) GDN_BAD_ARG("dt, dx, dy must be positive");
   return GDN_OK;
 }
 
+
 template <typename T>
 static int run(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuffers* b,
                cudaStream_t stream) {
-  using A_f = float;
   int st = validate(p, pts, b);
   if (st) return st;
   const Layout L = make_layout(p, sizeof(T));
@@ -533,11 +659,11 @@ static int run(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuffers*
   d.R = L.R;
   d.n_steps = N;
   d.n_freq = p->n_freq;
-  d.tiles_x = L.tiles_x;
+  d.plane = L.plane;
   d.slot = L.slot;
   d.ring = reinterpret_cast<T*>(ws + L.ring);
-  d.ca = static_cast<const T*>(b->ca);
-  d.cb = static_cast<const T*>(b->cb);
+  d.ca = reinterpret_cast<const T*>(ws + L.ca);
+  d.cb = reinterpret_cast<const T*>(ws + L.cb);
   d.eps = static_cast<const T*>(b->eps);
   d.ikx_e = static_cast<const T*>(b->inv_kx_e);
   d.iky_e = static_cast<const T*>(b->inv_ky_e);
@@ -549,10 +675,16 @@ static int run(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuffers*
   GDN_TAB(b_hyx_lo); GDN_TAB(c_hyx_lo); GDN_TAB(b_hyx_hi); GDN_TAB(c_hyx_hi);
   GDN_TAB(b_hxy_lo); GDN_TAB(c_hxy_lo); GDN_TAB(b_hxy_hi); GDN_TAB(c_hxy_hi);
 #undef GDN_TAB
-  T* psi[8];
-  for (int k = 0; k < 8; ++k) psi[k] = reinterpret_cast<T*>(ws + L.psi[k]);
-  d.ezx_lo = psi[0]; d.ezx_hi = psi[1]; d.ezy_lo = psi[2]; d.ezy_hi = psi[3];
-  d.hyx_lo = psi[4]; d.hyx_hi = psi[5]; d.hxy_lo = psi[6]; d.hxy_hi = psi[7];
+  d.ezx_lo = reinterpret_cast<T*>(ws + L.psi_e[0]);
+  d.ezx_hi = reinterpret_cast<T*>(ws + L.psi_e[1]);
+  d.ezy_lo = reinterpret_cast<T*>(ws + L.psi_e[2]);
+  d.ezy_hi = reinterpret_cast<T*>(ws + L.psi_e[3]);
+  for (int par = 0; par < 2; ++par) {
+    d.hyx_lo[par] = reinterpret_cast<T*>(ws + L.psi_h[0 + par]);
+    d.hyx_hi[par] = reinterpret_cast<T*>(ws + L.psi_h[2 + par]);
+    d.hxy_lo[par] = reinterpret_cast<T*>(ws + L.psi_h[4 + par]);
+    d.hxy_hi[par] = reinterpret_cast<T*>(ws + L.psi_h[6 + par]);
+  }
   d.dt_mu = T(b->dt_mu);
   d.inv_dx = T(b->inv_dx);
   d.inv_dy = T(b->inv_dy);
@@ -583,66 +715,70 @@ static int run(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuffers*
   int* step_base = reinterpret_cast<int*>(ws + L.step);
   d.step_base = step_base;
 
-  // Bin the point lists by tile and upload them.
+  // Bin the point lists by tile and upload them (pageable copies are staged
+  // before cudaMemcpyAsync returns, so the host vectors may go out of scope).
   const int counts[5] = {p->n_sources, p->n_ports, p->n_mx, p->n_my, p->n_probes};
   const int32_t* is[5] = {pts->src_i, pts->port_i, pts->mx_i, pts->my_i, pts->probe_i};
   const int32_t* js[5] = {pts->src_j, pts->port_j, pts->mx_j, pts->my_j, pts->probe_j};
+  const int kinds[5] = {0, 0, 1, 2, 0};
   const int* offs[5];
-  const int2* pls[5];
+  const Pt* pls[5];
   for (int k = 0; k < 5; ++k) {
-    PointBins pb = bin_points(counts[k], is[k], js[k], TI, TJ, L.tiles_x, L.n_tiles, L.ld);
-    GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.off[k], pb.off.data(), pb.off.size() * sizeof(int),
+    Bins bn = bin_tiles(counts[k], is[k], js[k], L, kinds[k]);
+    GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.off[k], bn.off.data(), bn.off.size() * sizeof(int),
                                  cudaMemcpyHostToDevice, stream));
-    if (counts[k] > 0)
-      GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.pts[k], pb.pts.data(), pb.pts.size() * sizeof(int2),
+    if (!bn.pts.empty())
+      GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.pts[k], bn.pts.data(), bn.pts.size() * sizeof(Pt),
                                    cudaMemcpyHostToDevice, stream));
     offs[k] = reinterpret_cast<const int*>(ws + L.off[k]);
-    pls[k] = reinterpret_cast<const int2*>(ws + L.pts[k]);
+    pls[k] = reinterpret_cast<const Pt*>(ws + L.pts[k]);
   }
-  // Pageable host vectors above are staged by the copy before it returns.
   d.src_off = offs[0]; d.src_pts = pls[0];
   d.port_off = offs[1]; d.port_pts = pls[1];
   d.mx_off = offs[2]; d.mx_pts = pls[2];
   d.my_off = offs[3]; d.my_pts = pls[3];
   d.probe_off = offs[4]; d.probe_pts = pls[4];
 
-  // Zero the state: ring, psi, counter, energy accumulators, DFT outputs.
-  GDN_TRY_CUDA(cudaMemsetAsync(ws + L.ring, 0, size_t(L.R) * L.slot * sizeof(T), stream));
-  // The eight psi slabs are carved back to back, ending where off[0] starts.
-  GDN_TRY_CUDA(cudaMemsetAsync(ws + L.psi[0], 0, L.off[0] - L.psi[0], stream));
+  // Zero the state (ring, padded ca/cb, psi, counter, energy) and pad ca/cb in.
+  GDN_TRY_CUDA(cudaMemsetAsync(ws + L.ring, 0, L.psi_end - L.ring, stream));
   GDN_TRY_CUDA(cudaMemsetAsync(step_base, 0, sizeof(int), stream));
+  const int eblocks = int(std::min<long long>(div_up((long long)nx * ny, 256), 148 * 8));
+  tm_pad_in<T><<<eblocks, 256, 0, stream>>>(static_cast<const T*>(b->ca),
+                                             reinterpret_cast<T*>(ws + L.ca), nx, ny, L.ld);
+  tm_pad_in<T><<<eblocks, 256, 0, stream>>>(static_cast<const T*>(b->cb),
+                                             reinterpret_cast<T*>(ws + L.cb), nx, ny, L.ld);
   double* eacc = reinterpret_cast<double*>(ws + L.eacc);
   if (p->record_energy)
     GDN_TRY_CUDA(cudaMemsetAsync(eacc, 0, 2 * size_t(std::max(N, 1)) * sizeof(double), stream));
 
   const bool f64acc = p->dft_f64 != 0;
   const size_t csz = f64acc ? sizeof(double2) : sizeof(float2);
-  DftDev<float> qf{};
-  DftDev<double> qd{};
-  long long dft_counts[3] = {0, 0, 0};
-  void* const dft_out[3] = {b->dft_ez, b->dft_hx, b->dft_hy};
-  const int full_shape[3][2] = {{nx, ny}, {nx, ny - 1}, {nx - 1, ny}};
-  for (int c = 0; c < 3; ++c) {
-    int lo0 = 0, lo1 = 0, hi0 = full_shape[c][0], hi1 = full_shape[c][1];
-    if (p->use_dft_region) {
-      lo0 = p->dft_lo[c][0]; lo1 = p->dft_lo[c][1];
-      hi0 = p->dft_hi[c][0]; hi1 = p->dft_hi[c][1];
-      if (hi0 <= lo0 || hi1 <= lo1) { lo0 = lo1 = hi0 = hi1 = 0; }
+  std::vector<Mon> mons;
+  if (p->n_freq > 0) {
+    if (p->n_monitors == 0) {
+      void* const outs[3] = {b->dft_ez, b->dft_hx, b->dft_hy};
+      const int shp[3][2] = {{nx, ny}, {nx, ny - 1}, {nx - 1, ny}};
+      for (int c = 0; c < 3; ++c)
+        mons.push_back(Mon{c, 0, 0, shp[c][1], (long long)shp[c][0] * shp[c][1], outs[c]});
+    } else {
+      for (int k = 0; k < p->n_monitors; ++k) {
+        const GdnDftMonitor& m = pts->monitors[k];
+        const int h = m.hi[0] - m.lo[0], w = m.hi[1] - m.lo[1];
+        mons.push_back(Mon{m.comp, m.lo[0], m.lo[1], w, (long long)h * w, m.out});
+      }
     }
-    if (p->n_freq == 0) { lo0 = lo1 = hi0 = hi1 = 0; }
-    qf.lo[c][0] = qd.lo[c][0] = lo0; qf.lo[c][1] = qd.lo[c][1] = lo1;
-    qf.hi[c][0] = qd.hi[c][0] = hi0; qf.hi[c][1] = qd.hi[c][1] = hi1;
-    qf.acc[c] = static_cast<float2*>(dft_out[c]);
-    qd.acc[c] = static_cast<double2*>(dft_out[c]);
-    dft_counts[c] = (long long)(hi0 - lo0) * (hi1 - lo1);
-    if (dft_counts[c] > 0)
-      GDN_TRY_CUDA(cudaMemsetAsync(dft_out[c], 0, size_t(dft_counts[c]) * p->n_freq * csz, stream));
   }
-  const long long max_cells = std::max({dft_counts[0], dft_counts[1], dft_counts[2]});
+  long long max_cells = 0;
+  for (const Mon& m : mons) {
+    max_cells = std::max(max_cells, m.count);
+    GDN_TRY_CUDA(cudaMemsetAsync(m.out, 0, size_t(m.count) * p->n_freq * csz, stream));
+  }
+  const Mon* d_mons = reinterpret_cast<const Mon*>(ws + L.mons);
+  if (!mons.empty())
+    GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.mons, mons.data(), mons.size() * sizeof(Mon),
+                                 cudaMemcpyHostToDevice, stream));
 
-  const dim3 blk(TJ, TI);
   const dim3 grd(L.tiles_x, L.tiles_y);
-  const int eblocks = int(std::min<long long>(div_up((long long)nx * ny, 256), 148 * 8));
 
   // Capture one chunk of `cnt` steps as a graph.
   auto capture = [&](int cnt, cudaGraphExec_t* exec) -> int {
@@ -650,28 +786,27 @@ static int run(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuffers*
     if (!cs) GDN_BAD_ARG("no capture stream for this device");
     GDN_TRY_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
     for (int s = 0; s < cnt; ++s) {
-      tm_h_sweep<T><<<grd, blk, 0, cs>>>(d, s);
-      tm_e_sweep<T><<<grd, blk, 0, cs>>>(d, s);
+      tm_step<T><<<grd, NT, 0, cs>>>(d, s);
       if (p->record_energy) tm_energy<T><<<eblocks, 256, 0, cs>>>(d, eacc, s);
     }
-    if (p->n_freq > 0 && max_cells > 0) {
-      const dim3 dg(unsigned(div_up(max_cells, 256)), 3);
+    if (!mons.empty()) {
+      const dim3 dg(unsigned(div_up(max_cells, 256)), unsigned(mons.size()));
       if (f64acc) {
         const size_t sm = size_t(4) * cnt * p->n_freq * sizeof(double);
-        tm_dft_fold<T, double><<<dg, 256, sm, cs>>>(d, qd, 0, cnt);
+        tm_dft_fold<T, double><<<dg, 256, sm, cs>>>(d, d_mons, 0, cnt);
       } else {
         const size_t sm = size_t(4) * cnt * p->n_freq * sizeof(float);
-        tm_dft_fold<T, A_f><<<dg, 256, sm, cs>>>(d, qf, 0, cnt);
+        tm_dft_fold<T, float><<<dg, 256, sm, cs>>>(d, d_mons, 0, cnt);
       }
     }
     tm_advance<<<1, 1, 0, cs>>>(step_base, cnt);
     cudaGraph_t g = nullptr;
-    cudaError_t e1 = cudaStreamEndCapture(cs, &g);
+    const cudaError_t e1 = cudaStreamEndCapture(cs, &g);
     if (e1 != cudaSuccess) {
       set_error("graph capture failed: %s", cudaGetErrorString(e1));
       return GDN_ERR_CUDA;
     }
-    cudaError_t e2 = cudaGraphInstantiate(exec, g, 0);
+    const cudaError_t e2 = cudaGraphInstantiate(exec, g, 0);
     cudaGraphDestroy(g);
     if (e2 != cudaSuccess) {
       set_error("graph instantiate failed: %s", cudaGetErrorString(e2));
@@ -700,16 +835,15 @@ static int run(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuffers*
 
   // Finalise: fields out, DFT x dt (fdtd2d.py:482-487), energy.
   const T* last = d.ring + (long long)(N % L.R) * L.slot;
-  tm_copy_out<T><<<eblocks, 256, 0, stream>>>(last, nx, ny, L.ld, static_cast<T*>(b->ez),
-                                                  static_cast<T*>(b->hx), static_cast<T*>(b->hy));
-  for (int c = 0; c < 3; ++c) {
-    if (dft_counts[c] <= 0 || p->n_freq == 0) continue;
-    const long long cnt = dft_counts[c] * p->n_freq;
+  tm_copy_out<T><<<eblocks, 256, 0, stream>>>(last, L.plane, nx, ny, L.ld, static_cast<T*>(b->ez),
+                                              static_cast<T*>(b->hx), static_cast<T*>(b->hy));
+  for (const Mon& m : mons) {
+    const long long cnt = m.count * p->n_freq;
     const int blocks = int(std::min<long long>(div_up(cnt, 256), 148 * 8));
     if (f64acc)
-      tm_dft_scale<double2><<<blocks, 256, 0, stream>>>(static_cast<double2*>(dft_out[c]), cnt, p->dt);
+      tm_dft_scale<double2><<<blocks, 256, 0, stream>>>(static_cast<double2*>(m.out), cnt, p->dt);
     else
-      tm_dft_scale<float2><<<blocks, 256, 0, stream>>>(static_cast<float2*>(dft_out[c]), cnt, p->dt);
+      tm_dft_scale<float2><<<blocks, 256, 0, stream>>>(static_cast<float2*>(m.out), cnt, p->dt);
   }
   if (p->record_energy && N > 0)
     tm_energy_finish<T><<<unsigned(div_up(N, 256)), 256, 0, stream>>>(

@@ -69,6 +69,7 @@ class SimResult(NamedTuple):
     dft_ez: torch.Tensor | None = None
     dft_hx: torch.Tensor | None = None
     dft_hy: torch.Tensor | None = None
+    monitors: list | None = None
 
 
 def field_energy(ez, hx, hy, eps, grid: Grid2D):
@@ -187,6 +188,7 @@ def simulate_tm(
     dtype=None,
     device=None,
     dft_region=None,
+    dft_monitors=None,
     cw_sources=None,
 ) -> SimResult:
     """Run a 2D TM FDTD simulation on the GPU (drop-in for fdtd2d.simulate_tm).
@@ -202,7 +204,9 @@ def simulate_tm(
     Additions: ``dtype`` forces the field dtype; ``device`` selects the CUDA
     device; ``dft_region`` = (ez_rect, hx_rect, hy_rect), each
     (lo_i, lo_j, hi_i, hi_j) or None, limits the DFT to those rectangles;
-    ``cw_sources`` = dict(env, src_w, mx_w, my_w) synthesises the Jz/Mx/My
+    ``dft_monitors`` = [(comp, lo_i, lo_j, hi_i, hi_j), ...] with comp 0/1/2 =
+    ez/hx/hy records only those boxes (returned in ``SimResult.monitors``,
+    dft_ez/hx/hy are then None); ``cw_sources`` = dict(env, src_w, mx_w, my_w) synthesises the Jz/Mx/My
     waveforms on the device as env[n] Re(sum_k W_k exp(+i w_k t_n)) (the
     frequency-domain adjoint's CW drive) instead of reading tabulated ones.
     """
@@ -347,18 +351,29 @@ def simulate_tm(
         raise ValueError("cw_sources needs dft_freqs")
 
     full_shapes = ((nx, ny), (nx, ny - 1), (nx - 1, ny))
-    rects = [None, None, None]
+    # Monitor list: (comp, rect) pairs; full grid when nothing is requested.
+    mon_specs = []
     if n_freq:
+        if dft_monitors is not None:
+            for m in dft_monitors:
+                comp = int(m[0])
+                if comp not in (0, 1, 2):
+                    raise ValueError(f"monitor component {comp} not in 0..2")
+                mon_specs.append((comp, _region_rect(m[1:5], full_shapes[comp])))
+        elif dft_region is not None:
+            for comp, (r, shp) in enumerate(zip(dft_region, full_shapes)):
+                rr = _region_rect(r, shp)
+                if rr is not None:
+                    mon_specs.append((comp, rr))
+    mon_out = [torch.empty((n_freq, r[2] - r[0], r[3] - r[1]), dtype=cdt, device=dev)
+               for _, r in mon_specs]
+    dft_out = [None, None, None]
+    if n_freq and dft_monitors is None:
         if dft_region is None:
-            rects = [(0, 0, s[0], s[1]) for s in full_shapes]
+            dft_out = [torch.empty((n_freq,) + s_, dtype=cdt, device=dev) for s_ in full_shapes]
         else:
-            rects = [_region_rect(r, s) for r, s in zip(dft_region, full_shapes)]
-    dft_out = []
-    for r in rects:
-        if r is None:
-            dft_out.append(None)
-        else:
-            dft_out.append(torch.empty((n_freq, r[2] - r[0], r[3] - r[1]), dtype=cdt, device=dev))
+            for (comp, _), t in zip(mon_specs, mon_out):
+                dft_out[comp] = t
 
     # Outputs.
     ez = torch.empty((nx, ny), dtype=fdt, device=dev)
@@ -379,8 +394,11 @@ def simulate_tm(
             w = cw_sources.get(key)
             if n == 0:
                 return None
-            w = torch.as_tensor(np.asarray(w), dtype=torch.complex128, device=dev).reshape(n, n_freq)
-            return w.contiguous()
+            if isinstance(w, torch.Tensor):
+                w = w.detach().to(device=dev, dtype=torch.complex128)
+            else:
+                w = torch.as_tensor(np.asarray(w), dtype=torch.complex128, device=dev)
+            return w.reshape(n, n_freq).contiguous()
 
         cw = dict(env=env, src_w=wts("src_w", src_idx.shape[0]), mx_w=wts("mx_w", mx_idx.shape[0]),
                   my_w=wts("my_w", my_idx.shape[0]))
@@ -393,11 +411,16 @@ def simulate_tm(
     params.record_energy = int(bool(record_energy))
     params.dft_f64 = int(cdt == torch.complex128)
     params.cw_sources = int(cw is not None)
-    params.use_dft_region = int(dft_region is not None)
-    for c, r in enumerate(rects):
-        if r is not None:
-            params.dft_lo[c][0], params.dft_lo[c][1] = r[0], r[1]
-            params.dft_hi[c][0], params.dft_hi[c][1] = r[2], r[3]
+    use_mons = bool(n_freq) and (dft_monitors is not None or dft_region is not None)
+    params.n_monitors = len(mon_specs) if use_mons else 0
+    mon_arr = (_native.DftMonitor * max(len(mon_specs), 1))()
+    for k, ((comp, r), t) in enumerate(zip(mon_specs, mon_out)):
+        mon_arr[k].comp = comp
+        mon_arr[k].lo[0], mon_arr[k].lo[1], mon_arr[k].lo[2] = r[0], r[1], 0
+        mon_arr[k].hi[0], mon_arr[k].hi[1], mon_arr[k].hi[2] = r[2], r[3], 1
+        mon_arr[k].out = t.data_ptr()
+    if use_mons and not mon_specs and cw_sources is None:
+        params.n_freq = 0  # every requested box is empty: no DFT work at all
     params.dt, params.dx, params.dy, params.dz, params.mu0 = dt, grid.dx, grid.dy, DZ, MU0
 
     idx_arrays = {
@@ -413,6 +436,7 @@ def simulate_tm(
     for k, (a, b) in cols.items():
         setattr(pts, f"{k}_i", _i32(a))
         setattr(pts, f"{k}_j", _i32(b))
+    pts.monitors = mon_arr
 
     bufs = _native.TmBuffers()
     bufs.ca, bufs.cb, bufs.eps = ca.data_ptr(), cb.data_ptr(), eps.data_ptr()
@@ -469,6 +493,7 @@ def simulate_tm(
         dft_ez=dft_out[0],
         dft_hx=dft_out[1],
         dft_hy=dft_out[2],
+        monitors=mon_out if dft_monitors is not None else None,
     )
 
 

@@ -79,15 +79,23 @@ typedef struct GdnTmParams {
   int32_t dft_f64;         /* 1: complex128 accumulators, 0: complex64        */
   int32_t cw_sources;      /* 1: Jz/Mx/My waveforms synthesised on the device
                               from per-source CW phasor weights (see buffers) */
-  int32_t use_dft_region;  /* 0: full-grid DFT; 1: per-component rectangles   */
-  /* Per-component DFT rectangles [lo, hi) in each component's own index
-   * space, order ez, hx, hy; used when use_dft_region = 1. An empty
-   * rectangle (hi <= lo on either axis) means "not accumulated". */
-  int32_t dft_lo[3][2];
-  int32_t dft_hi[3][2];
+  int32_t n_monitors;      /* 0: full-grid DFT into dft_ez/hx/hy; >0: only the
+                              boxes listed in GdnTmPoints.monitors             */
   double dt, dx, dy, dz;   /* dz = unit length of the 2D slice (DZ = 1 m)     */
   double mu0;              /* vacuum permeability used by the energy record   */
 } GdnTmParams;
+
+/* A running-DFT monitor: the box [lo, hi) of one field component, in that
+ * component's own index space (2D uses the first two axes). `out` is a
+ * DEVICE buffer of n_freq x box-shape complex values (complex64 or
+ * complex128 per dft_f64), written already scaled by dt. Region-limited
+ * monitors are the 2D/3D analogue of the reference's DFTRegions
+ * (src/gradenna/dft_region.py:37-92). */
+typedef struct GdnDftMonitor {
+  int32_t comp;            /* 2D: 0 ez, 1 hx, 2 hy; 3D: 0..5 = ex ey ez hx hy hz */
+  int32_t lo[3], hi[3];
+  void* out;
+} GdnDftMonitor;
 
 /* Host-memory point lists (int32 pairs split into i and j arrays). */
 typedef struct GdnTmPoints {
@@ -96,6 +104,7 @@ typedef struct GdnTmPoints {
   const int32_t *mx_i, *mx_j;       /* n_mx, on the Hx grid (nx, ny-1)        */
   const int32_t *my_i, *my_j;       /* n_my, on the Hy grid (nx-1, ny)        */
   const int32_t *probe_i, *probe_j; /* n_probes, margin 0                     */
+  const GdnDftMonitor* monitors;    /* n_monitors (host array)                */
 } GdnTmPoints;
 
 /* Device buffers. Field-typed arrays are float for *_f32, double for *_f64.
@@ -146,6 +155,41 @@ int gdn_tm_run_f32(const GdnTmParams* p, const GdnTmPoints* pts,
                    const GdnTmBuffers* b, void* stream);
 int gdn_tm_run_f64(const GdnTmParams* p, const GdnTmPoints* pts,
                    const GdnTmBuffers* b, void* stream);
+
+/* ------------------------------------------------------------------------ */
+/* Objective reductions and the frequency-domain adjoint contraction (2D)   */
+/* ------------------------------------------------------------------------ */
+
+/* Outward spectral Poynting flux through the dual-grid rectangle
+ * box = (il, ir, jb, jt) (replaces poynting_flux_box_2d,
+ * src/gradenna/monitors.py:20-70). dft_* are DEVICE complex phasors of the
+ * full-grid shapes (n_freq, nx, ny) / (n_freq, nx, ny-1) / (n_freq, nx-1, ny),
+ * complex128 when c128 = 1 else complex64; `out` is DEVICE double (n_freq). */
+int gdn_poynting_box_2d(int32_t nx, int32_t ny, int32_t n_freq, const int32_t box[4],
+                        double dx, double dy, int32_t c128, const void* dft_ez,
+                        const void* dft_hx, const void* dft_hy, double* out, void* stream);
+
+/* Cotangent of gdn_poynting_box_2d: ADDS g_out[k] * dP_k/dconj-phasor
+ * (torch's convention, dL/dRe + i dL/dIm) into g_ez / g_hx / g_hy, which have
+ * the shapes and complex type of the phasors. g_out is DEVICE double
+ * (n_freq). Deterministic (faces are processed in a fixed order). */
+int gdn_poynting_box_2d_grad(int32_t nx, int32_t ny, int32_t n_freq, const int32_t box[4],
+                             double dx, double dy, int32_t c128, const void* dft_ez,
+                             const void* dft_hx, const void* dft_hy, const double* g_out,
+                             void* g_ez, void* g_hx, void* g_hy, void* stream);
+
+/* Design-cell gradient of the frequency-domain adjoint (replaces the numpy
+ * contraction of freq_adjoint_gradient, src/gradenna/freq_adjoint.py:454-493):
+ *   dL/dtheta = eps_r * sum_k k_norm Re[conj(lam_k) conj(G_k)],
+ *   G_k = dca E_k / z_k + dcb (E_k - ca E_k / z_k) / cb,  z_k = exp(i w_k dt),
+ * with the closed-form dca, dcb of freq_adjoint.py:186-206. All arrays are
+ * DEVICE: e_fwd, lam (n_freq, n_cells) complex128; eps_r, sigma (n_cells)
+ * double; z (n_freq) complex128; grad_sigma / grad_eps_r (n_cells) double,
+ * either may be NULL. */
+int gdn_tm_adjoint_contract(int32_t n_cells, int32_t n_freq, double dt, double k_norm,
+                            const void* e_fwd, const void* lam, const double* eps_r,
+                            const double* sigma, const void* z, double* grad_sigma,
+                            double* grad_eps_r, void* stream);
 
 #ifdef __cplusplus
 }
