@@ -1,0 +1,439 @@
+#!/usr/bin/env python
+"""Benchmark: large 2D TM FDTD forward+adjoint design gradient on B200.
+
+Workload (one "step" = one full design-gradient evaluation):
+  Grid2D 1024 x 1024 at 1 mm, CPML 16, 8000 time steps, float32 fields;
+  512 x 512 design region [256:768, 256:768] with a seeded density
+  tanh_projection(conic_filter(U(0,1) noise, 3), beta=8, eta=0.5) mapped by
+  sigma_from_density; two 50-ohm RVS ports at (200, 512) (driven, a 4-tone
+  CW drive with a 300-step ramp) and (824, 512) (passive load); running DFT
+  at 4 frequencies over 2.0-3.0 GHz (complex128 accumulators); objective =
+  sum_k P_rad,k (Poynting box (150, 873, 150, 873)) - sum_k |S11_k|^2; its
+  gradient over all 512^2 design cells by the frequency-domain adjoint
+  (forward run + cotangents + adjoint run + contraction).
+  Synthetic inputs (no dataset exists for this workload).
+
+Metric: Gcell-steps/s fwd+adjoint = 2 * nx * ny * n_steps / time per step.
+
+  value   device-resident inputs, CUDA events per step on the launching
+          stream, L2 flushed (256 MiB write) before every timed step.
+  e2e     the same through the public API from pinned HOST inputs: the
+          design conductivity and the drive waveform are copied in, the
+          gradient is read back, inside the timed region.
+  roofline  dominant kernel tm_step: algorithmic bytes per launch (32 B per
+          cell for float32: Ez, Hx, Hy read + write, ca, cb read) / its mean
+          launch duration measured with CUDA events on a fields-only run of
+          the same grid; peak = MEASURED_PEAKS.json hbm_gbs.
+  cpu_baseline  the C oracle (restatement of the reference time loop, all
+          host threads) on a bounded sample of the same workload.
+
+Multi-GPU: one process per GPU (torchrun); every rank evaluates the gradient
+of its own seeded design (a population member) - no data-path collective;
+"scaling": "weak"; value = all ranks' cell-steps / max-over-ranks time.
+
+--impl reference: times the reference algorithm's CPU implementation here
+(the C oracle port; the reference's own JAX/Rust paths cannot run on this
+image) on the same config, each step a bounded sample; rank 0 only.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+N_GRID = 1024
+N_STEPS = 8000
+NPML = 16
+FREQS = tuple(np.linspace(2.0e9, 3.0e9, 4))
+DESIGN = (slice(256, 768), slice(256, 768))
+PORTS = ((200, 512), (824, 512))
+BOX = (150, 873, 150, 873)
+RAMP = 300
+RS = 50.0
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    ap.add_argument("--dtype", choices=("f32", "f64"), default="f32")
+    ap.add_argument("--grid", type=int, default=N_GRID)
+    ap.add_argument("--time-steps", type=int, default=N_STEPS)
+    return ap.parse_args()
+
+
+def workload(seed: int, n_grid: int, n_steps: int):
+    """Host (numpy) inputs of the workload for design `seed`."""
+    import torch
+
+    from gradenna_b200.grid import Grid2D
+    from gradenna_b200.materials import sigma_from_density
+    from gradenna_b200.topopt import seeded_density
+
+    grid = Grid2D(n_grid, n_grid, 1e-3, 1e-3)
+    s = n_grid / N_GRID
+    design = tuple(slice(int(a.start * s), int(a.stop * s)) for a in DESIGN)
+    shape = tuple(a.stop - a.start for a in design)
+    rho = seeded_density(shape, seed=seed, radius_cells=3.0, beta=8.0, eta=0.5,
+                         device="cpu", dtype=torch.float64).numpy()
+    sigma_d = np.asarray(sigma_from_density(rho), np.float64)
+    n = np.arange(n_steps)
+    env = np.clip(n / float(RAMP), 0.0, 1.0)
+    vs = env * sum(np.sin(2 * np.pi * f * (n + 0.5) * grid.dt) for f in FREQS)
+    ports = tuple((int(i * s), int(j * s)) for i, j in PORTS)
+    box = tuple(int(v * s) for v in BOX)
+    return dict(grid=grid, design=design, sigma_d=sigma_d, env=env, vs=vs, ports=ports, box=box)
+
+
+def make_objective(grid, box):
+    from gradenna_b200.monitors import poynting_flux_box_2d
+    from gradenna_b200.sparams import s11_power_wave
+
+    def obj(ph):
+        p = poynting_flux_box_2d(ph.dft_ez, ph.dft_hx, ph.dft_hy, grid, box)
+        s = s11_power_wave(ph.port_v[:, 0], ph.port_i[:, 0], RS)
+        return p.sum() - (s.real**2 + s.imag**2).sum()
+
+    return obj
+
+
+def monitors_for(w):
+    from gradenna_b200.monitors import port_monitors, poynting_box_monitors
+
+    mons = poynting_box_monitors(w["box"])
+    for p in w["ports"]:
+        mons += port_monitors(p)
+    return mons
+
+
+def gradient_call(w, sigma_dev, vs_dev, dtype, mons):
+    import gradenna_b200 as gb
+    from gradenna_b200.freq_adjoint import freq_adjoint_gradient
+
+    grid = w["grid"]
+    ports = (gb.Port(w["ports"][0], RS, vs_dev), gb.Port(w["ports"][1], RS, None))
+    return freq_adjoint_gradient(
+        grid, make_objective(grid, w["box"]), design_sigma=sigma_dev, design_region=w["design"],
+        dft_freqs=FREQS, env=w["env"], ports=ports, cpml=gb.CPMLSpec(NPML), dtype=dtype,
+        objective_monitors=mons)["sigma"]
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the C oracle on a bounded sample of the workload
+# ---------------------------------------------------------------------------
+
+
+def cpu_sample(w, dtype_np, target_s: float = 10.0):
+    """Time forward + adjoint-shaped C-oracle runs of n_s steps on the full
+    grid (all host threads); n_s is sized so the sample takes ~target_s."""
+    from oracle import fdtd2d_np as onp
+    from oracle.tm2d_c import simulate_tm_c
+
+    g = w["grid"]
+    og = onp.Grid2D(g.nx, g.ny, g.dx, g.dy)
+    sigma = np.zeros((g.nx, g.ny))
+    sigma[w["design"]] = w["sigma_d"]
+    (a0, a1), (b0, b1) = [(s.start, s.stop) for s in w["design"]]
+    mons = [(0, a0, b0, a1, b1)] + monitors_for(w)
+
+    def run(n_s):
+        kw = dict(sigma=sigma, ports=(onp.Port(w["ports"][0], RS, w["vs"][:n_s]),
+                                      onp.Port(w["ports"][1], RS, None)),
+                  dft_freqs=FREQS, cpml=onp.CPMLSpec(NPML), dtype=dtype_np, dft_monitors=mons)
+        t0 = time.perf_counter()
+        simulate_tm_c(og, **kw)  # forward run
+        simulate_tm_c(og, **kw)  # adjoint-shaped run (same stencil work)
+        return time.perf_counter() - t0
+
+    probe = 10
+    t = run(probe)
+    n_s = int(np.clip(target_s / max(t, 1e-6) * probe, 20, len(w["vs"])))
+    t = run(n_s)
+    cells = g.nx * g.ny
+    return 2 * cells * n_s / t / 1e9, n_s, t
+
+
+# ---------------------------------------------------------------------------
+# helpers
+# ---------------------------------------------------------------------------
+
+
+class ClockSampler:
+    """nvidia-smi clock / throttle sampling during the timed region."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        self.out = ""
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=10)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                self.out = ""
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in (self.out or "").splitlines():
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": mx, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peak():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except (OSError, KeyError, ValueError):
+        return 6650.0, "fallback"
+
+
+def profiled_traffic():
+    """dram bytes per tm_step launch from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", "tm_step_1024.md")
+    try:
+        for line in open(path):
+            if line.startswith("traffic_bytes_per_launch:"):
+                return int(float(line.split(":", 1)[1]))
+    except OSError:
+        pass
+    return None
+
+
+def dist_setup(args):
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# ---------------------------------------------------------------------------
+# arms
+# ---------------------------------------------------------------------------
+
+
+def run_reference(args):
+    world, rank, _ = dist_setup(args)
+    if rank != 0:
+        return 0
+    w = workload(0, args.grid, args.time_steps)
+    dt_np = np.float32 if args.dtype == "f32" else np.float64
+    vals = []
+    n_s = None
+    for k in range(args.warmup + args.steps):
+        v, n_s, _ = cpu_sample(w, dt_np, target_s=6.0)
+        if k >= args.warmup:
+            vals.append(v)
+    value = float(np.mean(vals))
+    cores = os.cpu_count()
+    line = {
+        "impl": "reference", "metric": "Gcell-steps/s fwd+adjoint", "value": value,
+        "unit": "Gcell-steps/s", "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 2 * w["grid"].nx * w["grid"].ny * args.time_steps / value / 1e6,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": args.dtype,
+        "data": "synthetic",
+        "config": config_dict(args, w),
+        "cpu_baseline": {"value": value, "unit": "Gcell-steps/s", "cores": cores, "kind": "port",
+                         "sample": f"forward + adjoint-shaped runs of {n_s} of {args.time_steps} "
+                                   f"steps on the full {args.grid}^2 grid per step"},
+        "e2e": {"value": value, "unit": "Gcell-steps/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def config_dict(args, w):
+    g = w["grid"]
+    return {
+        "workload": f"2D TM {g.nx}x{g.ny} @1mm, CPML {NPML}, {args.time_steps} steps, 2 RVS ports, "
+                    f"K={len(FREQS)} DFT (complex128), P_rad - |S11|^2 objective, freq-adjoint "
+                    f"gradient over a {w['sigma_d'].shape[0]}x{w['sigma_d'].shape[1]} design",
+        "grid": [g.nx, g.ny], "time_steps": args.time_steps, "n_freq": len(FREQS),
+        "design_cells": int(w["sigma_d"].size), "parallelism": f"replicas x{args.gpus}",
+        "l2": "flushed (256 MiB write) before every timed step; ring working set > L2",
+    }
+
+
+def run_ours(args):
+    import torch
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=dev)
+        pg = dist
+
+    from gradenna_b200 import _native
+
+    fdt = torch.float32 if args.dtype == "f32" else torch.float64
+    w = workload(rank, args.grid, args.time_steps)
+    mons = monitors_for(w)
+    sigma_dev = torch.as_tensor(w["sigma_d"], device=dev)
+    vs_dev = torch.as_tensor(w["vs"], device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+
+    for _ in range(args.warmup):
+        gradient_call(w, sigma_dev, vs_dev, fdt, mons)
+    torch.cuda.synchronize()
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    times = []
+    barrier()
+    l0 = _native.kernel_launches()
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            g = gradient_call(w, sigma_dev, vs_dev, fdt, mons)
+            e1.record()
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1) / 1e3)
+    launches = (_native.kernel_launches() - l0) // args.steps
+    barrier()
+    t_step = float(np.mean(times))
+    assert torch.isfinite(g).all()
+
+    # e2e: public API from pinned host inputs, gradient read back.
+    sig_h = torch.as_tensor(w["sigma_d"]).pin_memory()
+    vs_h = torch.as_tensor(w["vs"]).pin_memory()
+    out_h = torch.empty(w["sigma_d"].shape, dtype=torch.float64).pin_memory()
+    e2e_times = []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        sd = sig_h.to(dev, non_blocking=True)
+        vd = vs_h.to(dev, non_blocking=True)
+        gg = gradient_call(w, sd, vd, fdt, mons)
+        out_h.copy_(gg, non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        e2e_times.append(e0.elapsed_time(e1) / 1e3)
+    t_e2e = float(np.mean(e2e_times))
+
+    # Dominant-kernel duration: fields-only run of the same grid and ports.
+    import gradenna_b200 as gb
+
+    n_probe = 2000
+    probe_ports = (gb.Port(w["ports"][0], RS, vs_dev[:n_probe]), gb.Port(w["ports"][1], RS, None))
+    gb.simulate_tm(w["grid"], ports=probe_ports, cpml=gb.CPMLSpec(NPML), dtype=fdt)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    gb.simulate_tm(w["grid"], ports=probe_ports, cpml=gb.CPMLSpec(NPML), dtype=fdt)
+    e1.record()
+    torch.cuda.synchronize()
+    t_kernel = e0.elapsed_time(e1) / 1e3 / n_probe
+
+    if pg is not None:
+        tt = torch.tensor([t_step, t_e2e], device=dev, dtype=torch.float64)
+        pg.all_reduce(tt, op=pg.ReduceOp.MAX)
+        t_step, t_e2e = float(tt[0]), float(tt[1])
+
+    g_ = w["grid"]
+    cell_steps = 2 * g_.nx * g_.ny * args.time_steps
+    value = world * cell_steps / t_step / 1e9
+    e2e = world * cell_steps / t_e2e / 1e9
+    esize = 4 if fdt == torch.float32 else 8
+    algo_bytes = 8 * esize * g_.nx * g_.ny
+    achieved = algo_bytes / t_kernel / 1e9
+    peak, peak_kind = measured_peak()
+    h2d = w["sigma_d"].nbytes + w["vs"].nbytes
+    d2h = w["sigma_d"].nbytes
+
+    cpu = None
+    if rank == 0:
+        v_cpu, n_s, t_cpu = cpu_sample(w, np.float32 if fdt == torch.float32 else np.float64)
+        cpu = {"value": v_cpu, "unit": "Gcell-steps/s", "cores": os.cpu_count(), "kind": "port",
+               "sample": f"C oracle, forward + adjoint-shaped runs of {n_s} steps on the full "
+                         f"{g_.nx}^2 grid ({t_cpu:.1f} s)"}
+    if rank == 0:
+        line = {
+            "metric": "Gcell-steps/s fwd+adjoint", "value": value, "unit": "Gcell-steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": args.dtype, "data": "synthetic",
+            "config": config_dict(args, w),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": profiled_traffic(),
+                         "kernel": "tm_step", "peak_source": peak_kind,
+                         "algorithmic_bytes_per_launch": algo_bytes,
+                         "launch_us": t_kernel * 1e6},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e, "unit": "Gcell-steps/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

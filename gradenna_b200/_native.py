@@ -89,6 +89,8 @@ def _configure(lib) -> None:
     lib.gdn_version.argtypes = []
     lib.gdn_last_error.restype = ctypes.c_char_p
     lib.gdn_last_error.argtypes = []
+    lib.gdn_kernel_launches.restype = ctypes.c_uint64
+    lib.gdn_kernel_launches.argtypes = []
     lib.gdn_tm_workspace_size.restype = ctypes.c_int
     lib.gdn_tm_workspace_size.argtypes = [
         ctypes.POINTER(TmParams), ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]
@@ -162,3 +164,8 @@ def require_cuda(device=None):
 def ptr(t) -> int | None:
     """Device pointer of a tensor (None for None)."""
     return None if t is None else t.data_ptr()
+
+
+def kernel_launches() -> int:
+    """Kernels this library has launched in this process (gdn_kernel_launches)."""
+    return int(load().gdn_kernel_launches())

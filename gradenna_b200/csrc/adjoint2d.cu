@@ -203,6 +203,7 @@ extern "C" int gdn_poynting_box_2d(int32_t nx, int32_t ny, int32_t n_freq, const
     poynting_kernel<float2><<<n_freq, 256, 0, s>>>(b, dx, dy, static_cast<const float2*>(dft_ez),
                                                    static_cast<const float2*>(dft_hx),
                                                    static_cast<const float2*>(dft_hy), out);
+  gdn::count_launches(1);
   GDN_TRY_CUDA(cudaGetLastError());
   return GDN_OK;
 }
@@ -229,6 +230,7 @@ extern "C" int gdn_poynting_box_2d_grad(int32_t nx, int32_t ny, int32_t n_freq,
         b, dx, dy, static_cast<const float2*>(dft_ez), static_cast<const float2*>(dft_hx),
         static_cast<const float2*>(dft_hy), g_out, static_cast<float2*>(g_ez),
         static_cast<float2*>(g_hx), static_cast<float2*>(g_hy));
+  gdn::count_launches(1);
   GDN_TRY_CUDA(cudaGetLastError());
   return GDN_OK;
 }
@@ -246,6 +248,7 @@ extern "C" int gdn_tm_adjoint_contract(int32_t n_cells, int32_t n_freq, double d
       n_cells, n_freq, dt, k_norm, static_cast<const double2*>(e_fwd),
       static_cast<const double2*>(lam), eps_r, sigma, static_cast<const double2*>(z), grad_sigma,
       grad_eps_r);
+  gdn::count_launches(1);
   GDN_TRY_CUDA(cudaGetLastError());
   return GDN_OK;
 }

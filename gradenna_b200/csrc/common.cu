@@ -1,4 +1,5 @@
 // Error reporting, version string and the per-device capture stream.
+#include <atomic>
 #include <mutex>
 
 #include "common.cuh"
@@ -18,6 +19,10 @@ void set_error(const char* fmt, ...) {
 
 const char* last_error() { return g_last_error.c_str(); }
 
+static std::atomic<uint64_t> g_launches{0};
+void count_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+uint64_t total_launches() { return g_launches.load(std::memory_order_relaxed); }
+
 cudaStream_t capture_stream() {
   static std::mutex mu;
   static cudaStream_t streams[64] = {};
@@ -34,3 +39,5 @@ cudaStream_t capture_stream() {
 extern "C" const char* gdn_version(void) { return "gradenna_b200 0.1 (sm_100a)"; }
 
 extern "C" const char* gdn_last_error(void) { return gdn::last_error(); }
+
+extern "C" uint64_t gdn_kernel_launches(void) { return gdn::total_launches(); }

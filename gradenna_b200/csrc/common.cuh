@@ -52,36 +52,9 @@ struct Carve {
   size_t bytes() const { return (off + 255) & ~size_t(255); }
 };
 
-// Tile binning of point lists (sources, ports, probes, ...): a CSR over the
-// tiles of a kernel's grid so each CTA finds the points it owns with two
-// loads. `cells` holds (point index, linear cell index) pairs.
-struct PointBins {
-  std::vector<int> off;    // n_tiles + 1
-  std::vector<int2> pts;   // sorted by tile, stable in point order
-};
-
-inline PointBins bin_points(int n, const int32_t* pi, const int32_t* pj,
-                            int tile_i, int tile_j, int tiles_j, int n_tiles,
-                            long long ld) {
-  PointBins b;
-  b.off.assign(n_tiles + 1, 0);
-  b.pts.resize(n);
-  std::vector<int> tile_of(n);
-  for (int m = 0; m < n; ++m) {
-    int t = (pi[m] / tile_i) * tiles_j + (pj[m] / tile_j);
-    tile_of[m] = t;
-    b.off[t + 1]++;
-  }
-  for (int t = 0; t < n_tiles; ++t) b.off[t + 1] += b.off[t];
-  std::vector<int> cur(b.off.begin(), b.off.end() - 1);
-  for (int m = 0; m < n; ++m) {
-    int2 v;
-    v.x = m;
-    v.y = int(pi[m] * ld + pj[m]);
-    b.pts[cur[tile_of[m]]++] = v;
-  }
-  return b;
-}
+// Count of kernels this library launched (see gdn_kernel_launches).
+void count_launches(uint64_t n);
+uint64_t total_launches();
 
 // A private non-blocking stream per device used only to capture graphs; the
 // captured graphs are launched on the caller's stream.

@@ -747,6 +747,7 @@ static int run(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuffers*
                                              reinterpret_cast<T*>(ws + L.ca), nx, ny, L.ld);
   tm_pad_in<T><<<eblocks, 256, 0, stream>>>(static_cast<const T*>(b->cb),
                                              reinterpret_cast<T*>(ws + L.cb), nx, ny, L.ld);
+  count_launches(2);
   double* eacc = reinterpret_cast<double*>(ws + L.eacc);
   if (p->record_energy)
     GDN_TRY_CUDA(cudaMemsetAsync(eacc, 0, 2 * size_t(std::max(N, 1)) * sizeof(double), stream));
@@ -823,9 +824,14 @@ static int run(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuffers*
     if (g_full) cudaGraphExecDestroy(g_full);
     return st;
   }
+  // Kernel nodes per chunk graph: steps (+ energy), DFT fold, counter advance.
+  auto nodes = [&](int cnt) -> uint64_t {
+    return uint64_t(cnt) * (p->record_energy ? 2 : 1) + (mons.empty() ? 0 : 1) + 1;
+  };
   cudaError_t le = cudaSuccess;
   for (int c = 0; c < full && le == cudaSuccess; ++c) le = cudaGraphLaunch(g_full, stream);
   if (rem > 0 && le == cudaSuccess) le = cudaGraphLaunch(g_rem, stream);
+  count_launches(uint64_t(full) * (full ? nodes(Tc) : 0) + (rem ? nodes(rem) : 0));
   if (g_full) cudaGraphExecDestroy(g_full);
   if (g_rem) cudaGraphExecDestroy(g_rem);
   if (le != cudaSuccess) {
@@ -845,6 +851,7 @@ static int run(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuffers*
     else
       tm_dft_scale<float2><<<blocks, 256, 0, stream>>>(static_cast<float2*>(m.out), cnt, p->dt);
   }
+  count_launches(1 + mons.size() + (p->record_energy && N > 0 ? 1 : 0));
   if (p->record_energy && N > 0)
     tm_energy_finish<T><<<unsigned(div_up(N, 256)), 256, 0, stream>>>(
         eacc, static_cast<T*>(b->out_energy), N, p->dx * p->dy, p->mu0);

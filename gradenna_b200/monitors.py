@@ -16,7 +16,8 @@ import torch
 from gradenna_b200 import _native
 from gradenna_b200.grid import Grid2D
 
-__all__ = ["poynting_flux_box_2d", "log_radiated_fraction"]
+__all__ = ["poynting_flux_box_2d", "log_radiated_fraction", "poynting_box_monitors",
+           "port_monitors"]
 
 _I32x4 = ctypes.c_int32 * 4
 _native.register("gdn_poynting_box_2d", ctypes.c_int, [
@@ -92,3 +93,25 @@ def poynting_flux_box_2d(dft_ez, dft_hx, dft_hy, grid: Grid2D, box):
 def log_radiated_fraction(p_rad, p_avail):
     """Scale-invariant objective log P_rad - log P_avail (monitors.py:73-103)."""
     return torch.log(torch.as_tensor(p_rad)) - torch.log(torch.as_tensor(p_avail))
+
+
+def poynting_box_monitors(box):
+    """DFT monitor boxes (comp, lo_i, lo_j, hi_i, hi_j) covering exactly the
+    phasors poynting_flux_box_2d reads: four Ez strips two cells wide, the
+    two Hy rows and the two Hx columns of the contour. Recording only these
+    (instead of full grids) is the 2D analogue of the reference's
+    ntff_box_regions (src/gradenna/dft_region.py:187-227)."""
+    il, ir, jb, jt = (int(v) for v in box)
+    return [
+        (0, il, jb + 1, il + 2, jt + 1), (0, ir, jb + 1, ir + 2, jt + 1),
+        (0, il + 1, jb, ir + 1, jb + 2), (0, il + 1, jt, ir + 1, jt + 2),
+        (2, il, jb + 1, il + 1, jt + 1), (2, ir, jb + 1, ir + 1, jt + 1),
+        (1, il + 1, jb, ir + 1, jb + 1), (1, il + 1, jt, ir + 1, jt + 1),
+    ]
+
+
+def port_monitors(ij):
+    """Monitor boxes covering what the port phasor rebuild reads at Ez cell
+    (i, j): Ez(i, j), Hy(i-1..i, j), Hx(i, j-1..j) (freq_adjoint.py:536-558)."""
+    i, j = (int(v) for v in ij)
+    return [(0, i, j, i + 1, j + 1), (2, i - 1, j, i + 1, j + 1), (1, i, j - 1, i + 1, j + 1)]

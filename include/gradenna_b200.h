@@ -59,6 +59,11 @@ const char* gdn_version(void);
 /* Message describing the last non-zero status returned on this thread. */
 const char* gdn_last_error(void);
 
+/* Number of this library's CUDA kernels launched so far in this process
+ * (graph replays count every kernel node they run). No reference
+ * counterpart: it lets callers and benchmarks attribute device work. */
+uint64_t gdn_kernel_launches(void);
+
 /* ------------------------------------------------------------------------ */
 /* 2D TM                                                                    */
 /* ------------------------------------------------------------------------ */
