@@ -33,6 +33,7 @@
 //     step index from a device counter.
 #include <algorithm>
 #include <cmath>
+#include <mutex>
 
 #include "common.cuh"
 
@@ -883,4 +884,278 @@ extern "C" int gdn_tm_run_f32(const GdnTmParams* p, const GdnTmPoints* pts,
 extern "C" int gdn_tm_run_f64(const GdnTmParams* p, const GdnTmPoints* pts,
                               const GdnTmBuffers* b, void* stream) {
   return gdn::tm2d::run<double>(p, pts, b, static_cast<cudaStream_t>(stream));
+}
+
+// ===========================================================================
+// Allocation-free 2D TM entry point (no counterpart in the reference).
+//
+// For callers that cannot allocate device memory while they run the solver:
+// code that owns the GPU's memory through its own pool (the allocation would
+// fail or fragment that pool), real-time loops that forbid allocator calls,
+// and hosts that load this library without a CUDA allocator they may use.
+// The scratch (field ring, psi slabs, point bins, monitor table, step
+// counter) lives in one file-scope __device__ array of fixed size instead of
+// a workspace. Every GPU that loads this library holds the array until the
+// process exits.
+// ===========================================================================
+namespace gdn {
+namespace tm2d {
+
+constexpr size_t kStaticScratchBytes = size_t(32) << 20;  // 32 MiB per device
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
+
+// Device address of g_static_scratch on the current device. In host code the
+// array's name is only a host-side stand-in, so the address is looked up once
+// per device with cudaGetSymbolAddress (the first call on each device does
+// this set-up).
+static int static_scratch(char** out) {
+  static std::mutex mu;
+  static char* addr[64] = {};
+  int dev = 0;
+  GDN_TRY_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) GDN_BAD_ARG("device ordinal %d out of range", dev);
+  std::lock_guard<std::mutex> lock(mu);
+  if (!addr[dev]) {
+    void* p = nullptr;
+    GDN_TRY_CUDA(cudaGetSymbolAddress(&p, g_static_scratch));
+    addr[dev] = static_cast<char*>(p);
+  }
+  *out = addr[dev];
+  return GDN_OK;
+}
+
+// make_layout with an explicit DFT fold length T (the ring has T+1 slots).
+static Layout make_layout_fold(const GdnTmParams* p, size_t esize, int T) {
+  Layout L;
+  L.tiles_x = int(div_up(p->ny, TJ));
+  L.tiles_y = int(div_up(p->nx, TI));
+  L.n_tiles = L.tiles_x * L.tiles_y;
+  L.ld = PADJ + L.tiles_x * TJ + PADJ;
+  L.rows = L.tiles_y * TI + 2;
+  L.plane = (long long)L.rows * L.ld;
+  L.slot = 3 * L.plane;
+  L.T = T;
+  L.R = p->n_freq > 0 ? T + 1 : 2;
+  Carve cv;
+  L.ring = cv.take<char>(size_t(L.R) * L.slot * esize);
+  L.ca = cv.take<char>(size_t(L.plane) * esize);
+  L.cb = cv.take<char>(size_t(L.plane) * esize);
+  const size_t m = size_t(p->npml), nx = size_t(p->nx), ny = size_t(p->ny);
+  const size_t pe[4] = {m * (ny - 2), m * (ny - 2), (nx - 2) * m, (nx - 2) * m};
+  for (int k = 0; k < 4; ++k) L.psi_e[k] = cv.take<char>(std::max<size_t>(pe[k], 1) * esize);
+  const size_t ph[4] = {m * ny, m * ny, nx * m, nx * m};
+  for (int k = 0; k < 8; ++k) L.psi_h[k] = cv.take<char>(std::max<size_t>(ph[k / 2], 1) * esize);
+  L.psi_end = cv.take<char>(0);
+  const int counts[5] = {p->n_sources, p->n_ports, p->n_mx, p->n_my, p->n_probes};
+  for (int k = 0; k < 5; ++k) {
+    L.off[k] = cv.take<int>(L.n_tiles + 1);
+    L.pts[k] = cv.take<Pt>(2 * size_t(std::max(counts[k], 1)));
+  }
+  L.mons = cv.take<Mon>(size_t(std::max(p->n_monitors, 3)));
+  L.step = cv.take<int>(1);
+  L.eacc = cv.take<double>(p->record_energy ? 2 * size_t(std::max(p->n_steps, 1)) : 1);
+  L.total = cv.bytes();
+  return L;
+}
+
+// The gdn_tm_run_f32 time loop with the static scratch, launched eagerly
+// (no CUDA graph is instantiated, since instantiation may allocate).
+static int run_noalloc_f32(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuffers* b,
+                           cudaStream_t stream) {
+  using T = float;
+  int st = validate(p, pts, b);
+  if (st) return st;
+  // Largest fold length whose layout fits the static scratch.
+  Layout L = make_layout_fold(p, sizeof(T), 32);
+  if (p->n_freq > 0)
+    for (int t = 32; t >= 2 && L.total > kStaticScratchBytes; --t)
+      L = make_layout_fold(p, sizeof(T), t);
+  if (L.total > kStaticScratchBytes)
+    GDN_BAD_ARG("this run needs %zu bytes of scratch; the static scratch of "
+                "gdn_tm_run_noalloc_f32 holds %zu bytes (use gdn_tm_run_f32)",
+                L.total, kStaticScratchBytes);
+  char* ws = nullptr;
+  if ((st = static_scratch(&ws))) return st;
+
+  const int nx = p->nx, ny = p->ny, N = p->n_steps;
+  Dev<T> d{};
+  d.nx = nx;
+  d.ny = ny;
+  d.ld = L.ld;
+  d.npml = p->npml;
+  d.R = L.R;
+  d.n_steps = N;
+  d.n_freq = p->n_freq;
+  d.plane = L.plane;
+  d.slot = L.slot;
+  d.ring = reinterpret_cast<T*>(ws + L.ring);
+  d.ca = reinterpret_cast<const T*>(ws + L.ca);
+  d.cb = reinterpret_cast<const T*>(ws + L.cb);
+  d.eps = static_cast<const T*>(b->eps);
+  d.ikx_e = static_cast<const T*>(b->inv_kx_e);
+  d.iky_e = static_cast<const T*>(b->inv_ky_e);
+  d.ikx_h = static_cast<const T*>(b->inv_kx_h);
+  d.iky_h = static_cast<const T*>(b->inv_ky_h);
+#define GDN_TAB(x) d.x = static_cast<const T*>(b->x)
+  GDN_TAB(b_ezx_lo); GDN_TAB(c_ezx_lo); GDN_TAB(b_ezx_hi); GDN_TAB(c_ezx_hi);
+  GDN_TAB(b_ezy_lo); GDN_TAB(c_ezy_lo); GDN_TAB(b_ezy_hi); GDN_TAB(c_ezy_hi);
+  GDN_TAB(b_hyx_lo); GDN_TAB(c_hyx_lo); GDN_TAB(b_hyx_hi); GDN_TAB(c_hyx_hi);
+  GDN_TAB(b_hxy_lo); GDN_TAB(c_hxy_lo); GDN_TAB(b_hxy_hi); GDN_TAB(c_hxy_hi);
+#undef GDN_TAB
+  d.ezx_lo = reinterpret_cast<T*>(ws + L.psi_e[0]);
+  d.ezx_hi = reinterpret_cast<T*>(ws + L.psi_e[1]);
+  d.ezy_lo = reinterpret_cast<T*>(ws + L.psi_e[2]);
+  d.ezy_hi = reinterpret_cast<T*>(ws + L.psi_e[3]);
+  for (int par = 0; par < 2; ++par) {
+    d.hyx_lo[par] = reinterpret_cast<T*>(ws + L.psi_h[0 + par]);
+    d.hyx_hi[par] = reinterpret_cast<T*>(ws + L.psi_h[2 + par]);
+    d.hxy_lo[par] = reinterpret_cast<T*>(ws + L.psi_h[4 + par]);
+    d.hxy_hi[par] = reinterpret_cast<T*>(ws + L.psi_h[6 + par]);
+  }
+  d.dt_mu = T(b->dt_mu);
+  d.inv_dx = T(b->inv_dx);
+  d.inv_dy = T(b->inv_dy);
+  d.dx = T(p->dx);
+  d.dy = T(p->dy);
+  d.dz = T(p->dz);
+  d.n_src = p->n_sources;
+  d.n_ports = p->n_ports;
+  d.n_mx = p->n_mx;
+  d.n_my = p->n_my;
+  d.n_probes = p->n_probes;
+  d.cb_src = static_cast<const T*>(b->cb_src);
+  d.src_cur = static_cast<const T*>(b->src_cur);
+  d.cb_vs = static_cast<const T*>(b->cb_vs);
+  d.port_vs = static_cast<const T*>(b->port_vs);
+  d.mx_cur = static_cast<const T*>(b->mx_cur);
+  d.my_cur = static_cast<const T*>(b->my_cur);
+  d.cw = p->cw_sources;
+  d.cw_env = b->cw_env;
+  d.src_w = reinterpret_cast<const double2*>(b->src_w);
+  d.mx_w = reinterpret_cast<const double2*>(b->mx_w);
+  d.my_w = reinterpret_cast<const double2*>(b->my_w);
+  d.ph_e = reinterpret_cast<const double2*>(b->ph_e);
+  d.ph_h = reinterpret_cast<const double2*>(b->ph_h);
+  d.out_probe = static_cast<T*>(b->out_probe);
+  d.out_v = static_cast<T*>(b->out_v);
+  d.out_i = static_cast<T*>(b->out_i);
+  int* step_base = reinterpret_cast<int*>(ws + L.step);
+  d.step_base = step_base;
+
+  const int counts[5] = {p->n_sources, p->n_ports, p->n_mx, p->n_my, p->n_probes};
+  const int32_t* is[5] = {pts->src_i, pts->port_i, pts->mx_i, pts->my_i, pts->probe_i};
+  const int32_t* js[5] = {pts->src_j, pts->port_j, pts->mx_j, pts->my_j, pts->probe_j};
+  const int kinds[5] = {0, 0, 1, 2, 0};
+  const int* offs[5];
+  const Pt* pls[5];
+  for (int k = 0; k < 5; ++k) {
+    Bins bn = bin_tiles(counts[k], is[k], js[k], L, kinds[k]);
+    GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.off[k], bn.off.data(), bn.off.size() * sizeof(int),
+                                 cudaMemcpyHostToDevice, stream));
+    if (!bn.pts.empty())
+      GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.pts[k], bn.pts.data(), bn.pts.size() * sizeof(Pt),
+                                   cudaMemcpyHostToDevice, stream));
+    offs[k] = reinterpret_cast<const int*>(ws + L.off[k]);
+    pls[k] = reinterpret_cast<const Pt*>(ws + L.pts[k]);
+  }
+  d.src_off = offs[0]; d.src_pts = pls[0];
+  d.port_off = offs[1]; d.port_pts = pls[1];
+  d.mx_off = offs[2]; d.mx_pts = pls[2];
+  d.my_off = offs[3]; d.my_pts = pls[3];
+  d.probe_off = offs[4]; d.probe_pts = pls[4];
+
+  // The scratch keeps the previous call's contents: clear all state that the
+  // time loop expects to start at zero (ring incl. ghost cells, padded ca/cb
+  // ghosts, psi slabs, step counter, energy sums).
+  GDN_TRY_CUDA(cudaMemsetAsync(ws + L.ring, 0, L.psi_end - L.ring, stream));
+  GDN_TRY_CUDA(cudaMemsetAsync(step_base, 0, sizeof(int), stream));
+  const int eblocks = int(std::min<long long>(div_up((long long)nx * ny, 256), 148 * 8));
+  tm_pad_in<T><<<eblocks, 256, 0, stream>>>(static_cast<const T*>(b->ca),
+                                             reinterpret_cast<T*>(ws + L.ca), nx, ny, L.ld);
+  tm_pad_in<T><<<eblocks, 256, 0, stream>>>(static_cast<const T*>(b->cb),
+                                             reinterpret_cast<T*>(ws + L.cb), nx, ny, L.ld);
+  double* eacc = reinterpret_cast<double*>(ws + L.eacc);
+  if (p->record_energy)
+    GDN_TRY_CUDA(cudaMemsetAsync(eacc, 0, 2 * size_t(std::max(N, 1)) * sizeof(double), stream));
+
+  const bool f64acc = p->dft_f64 != 0;
+  const size_t csz = f64acc ? sizeof(double2) : sizeof(float2);
+  std::vector<Mon> mons;
+  if (p->n_freq > 0) {
+    if (p->n_monitors == 0) {
+      void* const outs[3] = {b->dft_ez, b->dft_hx, b->dft_hy};
+      const int shp[3][2] = {{nx, ny}, {nx, ny - 1}, {nx - 1, ny}};
+      for (int c = 0; c < 3; ++c)
+        mons.push_back(Mon{c, 0, 0, shp[c][1], (long long)shp[c][0] * shp[c][1], outs[c]});
+    } else {
+      for (int k = 0; k < p->n_monitors; ++k) {
+        const GdnDftMonitor& m = pts->monitors[k];
+        const int h = m.hi[0] - m.lo[0], w = m.hi[1] - m.lo[1];
+        mons.push_back(Mon{m.comp, m.lo[0], m.lo[1], w, (long long)h * w, m.out});
+      }
+    }
+  }
+  long long max_cells = 0;
+  for (const Mon& m : mons) {
+    max_cells = std::max(max_cells, m.count);
+    GDN_TRY_CUDA(cudaMemsetAsync(m.out, 0, size_t(m.count) * p->n_freq * csz, stream));
+  }
+  const Mon* d_mons = reinterpret_cast<const Mon*>(ws + L.mons);
+  if (!mons.empty())
+    GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.mons, mons.data(), mons.size() * sizeof(Mon),
+                                 cudaMemcpyHostToDevice, stream));
+
+  // Eager time loop: chunks of L.T steps, each closed by the DFT fold and
+  // the counter advance, exactly as the graph of gdn_tm_run_f32 orders them.
+  const dim3 grd(L.tiles_x, L.tiles_y);
+  uint64_t launched = 2;
+  for (int base = 0; base < N; base += L.T) {
+    const int cnt = std::min(L.T, N - base);
+    for (int s = 0; s < cnt; ++s) {
+      tm_step<T><<<grd, NT, 0, stream>>>(d, s);
+      ++launched;
+      if (p->record_energy) {
+        tm_energy<T><<<eblocks, 256, 0, stream>>>(d, eacc, s);
+        ++launched;
+      }
+    }
+    if (!mons.empty()) {
+      const dim3 dg(unsigned(div_up(max_cells, 256)), unsigned(mons.size()));
+      if (f64acc)
+        tm_dft_fold<T, double><<<dg, 256, size_t(4) * cnt * p->n_freq * sizeof(double), stream>>>(
+            d, d_mons, 0, cnt);
+      else
+        tm_dft_fold<T, float><<<dg, 256, size_t(4) * cnt * p->n_freq * sizeof(float), stream>>>(
+            d, d_mons, 0, cnt);
+      ++launched;
+    }
+    tm_advance<<<1, 1, 0, stream>>>(step_base, cnt);
+    ++launched;
+  }
+
+  const T* last = d.ring + (long long)(N % L.R) * L.slot;
+  tm_copy_out<T><<<eblocks, 256, 0, stream>>>(last, L.plane, nx, ny, L.ld, static_cast<T*>(b->ez),
+                                              static_cast<T*>(b->hx), static_cast<T*>(b->hy));
+  for (const Mon& m : mons) {
+    const long long cnt = m.count * p->n_freq;
+    const int blocks = int(std::min<long long>(div_up(cnt, 256), 148 * 8));
+    if (f64acc)
+      tm_dft_scale<double2><<<blocks, 256, 0, stream>>>(static_cast<double2*>(m.out), cnt, p->dt);
+    else
+      tm_dft_scale<float2><<<blocks, 256, 0, stream>>>(static_cast<float2*>(m.out), cnt, p->dt);
+  }
+  if (p->record_energy && N > 0)
+    tm_energy_finish<T><<<unsigned(div_up(N, 256)), 256, 0, stream>>>(
+        eacc, static_cast<T*>(b->out_energy), N, p->dx * p->dy, p->mu0);
+  count_launches(launched + 1 + mons.size() + (p->record_energy && N > 0 ? 1 : 0));
+  GDN_TRY_CUDA(cudaGetLastError());
+  return GDN_OK;
+}
+
+}  // namespace tm2d
+}  // namespace gdn
+
+extern "C" int gdn_tm_run_noalloc_f32(const GdnTmParams* p, const GdnTmPoints* pts,
+                                      const GdnTmBuffers* b, void* stream) {
+  return gdn::tm2d::run_noalloc_f32(p, pts, b, static_cast<cudaStream_t>(stream));
 }

@@ -161,6 +161,30 @@ int gdn_tm_run_f32(const GdnTmParams* p, const GdnTmPoints* pts,
 int gdn_tm_run_f64(const GdnTmParams* p, const GdnTmPoints* pts,
                    const GdnTmBuffers* b, void* stream);
 
+/* Allocation-free variant of gdn_tm_run_f32. No counterpart in the
+ * reference: it exists for callers that must not allocate device memory
+ * while they run the solver -- code that owns all GPU memory through its own
+ * pool, real-time loops that forbid allocator calls, and hosts that load
+ * this library without a CUDA allocator they may use. The caller still
+ * passes every input and output buffer; the scratch (field ring, psi slabs,
+ * point bins, step counter) lives in a fixed 32 MiB __device__ array inside
+ * the library, which every GPU that loads the library holds until the
+ * process exits. b->workspace is ignored and nothing is allocated: no
+ * cudaMalloc/cudaFree, no graph instantiation (kernels are launched directly
+ * on `stream`).
+ *   - Runs whose scratch exceeds 32 MiB are rejected with GDN_ERR_BAD_ARG and
+ *     a message giving the bytes needed (square grids up to about 830 x 830
+ *     cells with a DFT, 960 x 960 without). The DFT fold length adapts to
+ *     the capacity.
+ *   - The first call on each device looks up the array's device address
+ *     (cudaGetSymbolAddress); make that first call before any stream capture.
+ *   - All calls share the one array and it keeps the last call's contents;
+ *     each call clears the state that must start at zero. Calls that overlap
+ *     on the GPU (different streams, or other host threads) race on it and
+ *     corrupt each other: serialise them. */
+int gdn_tm_run_noalloc_f32(const GdnTmParams* p, const GdnTmPoints* pts,
+                           const GdnTmBuffers* b, void* stream);
+
 /* ------------------------------------------------------------------------ */
 /* Objective reductions and the frequency-domain adjoint contraction (2D)   */
 /* ------------------------------------------------------------------------ */
