@@ -20,10 +20,12 @@ Metric: Gcell-steps/s fwd+adjoint = 2 * nx * ny * n_steps / time per step.
   e2e     the same through the public API from pinned HOST inputs: the
           design conductivity and the drive waveform are copied in, the
           gradient is read back, inside the timed region.
-  roofline  dominant kernel tm_step: algorithmic bytes per launch (32 B per
-          cell for float32: Ez, Hx, Hy read + write, ca, cb read) / its mean
-          launch duration measured with CUDA events on a fields-only run of
-          the same grid; peak = MEASURED_PEAKS.json hbm_gbs.
+  roofline  dominant kernel tm_tb (one launch = a block of TB = 4 time steps;
+          interior and boundary tiles run as two concurrent launches):
+          algorithmic bytes per block = TB x 32 B per cell for float32 (Ez, Hx,
+          Hy read + write, ca, cb read, per time step) / the block's mean
+          duration, measured with CUDA events on a fields-only run of the
+          same grid; peak = MEASURED_PEAKS.json hbm_gbs.
   cpu_baseline  the C oracle (restatement of the reference time loop, all
           host threads) on a bounded sample of the same workload.
 
@@ -232,8 +234,8 @@ def measured_peak():
 
 
 def profiled_traffic():
-    """dram bytes per tm_step launch from the committed ncu summary, or None."""
-    path = os.path.join(ROOT, "profiles", "tm_step_1024.md")
+    """dram bytes per tm_tb 4-step block from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", "tm_tb_1024.md")
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_launch:"):
@@ -391,8 +393,9 @@ def run_ours(args):
     value = world * cell_steps / t_step / 1e9
     e2e = world * cell_steps / t_e2e / 1e9
     esize = 4 if fdt == torch.float32 else 8
-    algo_bytes = 8 * esize * g_.nx * g_.ny
-    achieved = algo_bytes / t_kernel / 1e9
+    tb = 4
+    algo_bytes = tb * 8 * esize * g_.nx * g_.ny
+    achieved = algo_bytes / (tb * t_kernel) / 1e9
     peak, peak_kind = measured_peak()
     h2d = w["sigma_d"].nbytes + w["vs"].nbytes
     d2h = w["sigma_d"].nbytes
@@ -412,9 +415,9 @@ def run_ours(args):
             "config": config_dict(args, w),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": profiled_traffic(),
-                         "kernel": "tm_step", "peak_source": peak_kind,
+                         "kernel": "tm_tb (4-step block)", "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": algo_bytes,
-                         "launch_us": t_kernel * 1e6},
+                         "launch_us": tb * t_kernel * 1e6},
             "cpu_baseline": cpu,
             "e2e": {"value": e2e, "unit": "Gcell-steps/s", "h2d_bytes_per_step": int(h2d),
                     "d2h_bytes_per_step": int(d2h)},

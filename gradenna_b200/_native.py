@@ -93,7 +93,8 @@ def _configure(lib) -> None:
     lib.gdn_kernel_launches.argtypes = []
     lib.gdn_tm_workspace_size.restype = ctypes.c_int
     lib.gdn_tm_workspace_size.argtypes = [
-        ctypes.POINTER(TmParams), ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)]
+        ctypes.POINTER(TmParams), ctypes.POINTER(TmPoints), ctypes.c_int,
+        ctypes.POINTER(ctypes.c_size_t)]
     for name in ("gdn_tm_run_f32", "gdn_tm_run_f64"):
         fn = getattr(lib, name)
         fn.restype = ctypes.c_int

@@ -34,6 +34,17 @@ cudaStream_t capture_stream() {
   return streams[dev];
 }
 
+cudaStream_t capture_side_stream() {
+  static std::mutex mu;
+  static cudaStream_t streams[64] = {};
+  int dev = 0;
+  cudaGetDevice(&dev);
+  std::lock_guard<std::mutex> lock(mu);
+  if (dev < 0 || dev >= 64) return nullptr;
+  if (!streams[dev]) cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking);
+  return streams[dev];
+}
+
 }  // namespace gdn
 
 extern "C" const char* gdn_version(void) { return "gradenna_b200 0.1 (sm_100a)"; }

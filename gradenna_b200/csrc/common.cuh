@@ -59,6 +59,8 @@ uint64_t total_launches();
 // A private non-blocking stream per device used only to capture graphs; the
 // captured graphs are launched on the caller's stream.
 cudaStream_t capture_stream();
+// A second private stream per device for parallel branches inside captures.
+cudaStream_t capture_side_stream();
 
 template <typename T>
 struct Cplx;

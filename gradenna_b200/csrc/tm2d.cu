@@ -10,29 +10,33 @@
 //   injection and V record (:446-451) -> running DFT (:453-458) -> probes.
 //
 // B200 design:
-//   * One fused kernel per time step. A CTA owns a TI x TJ tile of Ez cells;
-//     it stages Ez^n, Hx, Hy for the tile plus a one-cell halo in shared
-//     memory with 16-byte cp.async copies, recomputes the halo row/column of
-//     H^{n+1/2} that its E update needs (instead of a second launch and a
-//     grid-wide dependency), updates E, applies the tile's point work
-//     (sources, ports, probes, magnetic currents) in shared memory and writes
-//     the tile back with 16-byte stores.
-//   * Field state lives in a RING of R slots (ez, hx, hy planes per slot).
-//     Step n reads slot n%R and writes slot (n+1)%R, so halo reads never race
-//     with the owner's writes, and every slot is a snapshot of the fields
-//     after one step. The running DFT is folded into the accumulators once
-//     per T = R-1 steps by one kernel that reads the T snapshots, so the
-//     accumulator read-modify-write traffic drops by T.
-//   * Planes are padded (one ghost row above/below, PADJ ghost columns on
-//     each side, rows a multiple of the tile) so every halo copy is aligned
-//     and in bounds; ghost cells stay zero, which is also the PEC ring.
-//   * H-type psi (updated redundantly on halo cells) is double-buffered by
-//     step parity; E-type psi is updated only by its owner, in place.
-//   * One chunk of T steps (T step kernels + DFT fold + counter advance) is
+//   * Temporal blocking. One launch advances TB time steps. A CTA owns a
+//     TI x TJ tile of cells and stages Ez, Hx, Hy, ca and cb for the tile plus
+//     a halo (TB rows, HJ >= TB columns) in shared memory with 16-byte
+//     cp.async copies, then runs the TB sub-steps entirely in shared memory:
+//     each sub-step's H and E sweeps also cover the halo (redundantly with the
+//     neighbours), whose valid part shrinks by one cell per sub-step, so the
+//     owned tile stays exact. Global traffic and launches drop by TB.
+//   * Field state is a ping-pong pair of padded planes (ghost rows/columns
+//     stay zero: they are also the PEC ring); launch k reads pair k&1 and
+//     writes pair (k+1)&1, so halo reads never race with owners' writes.
+//   * CPML psi lives in slab storage in HBM (double-buffered by launch
+//     parity). PML tiles copy the psi of their whole extended region into a
+//     private HBM buffer, advance it across the sub-steps and write back the
+//     owned cells, so halo recomputation never touches shared state.
+//   * Point work (sources, ports, probes, magnetic currents) is binned on the
+//     host into per-tile lists that include the halo; injections are applied
+//     to every copy of a cell, records (V, I, probes) only by the owner.
+//   * The running DFT reads a compact MONITOR RING: every sub-step the owner
+//     writes the monitored cells' values (only those) into ring slot n % R;
+//     once per R steps one fold kernel adds sum_t ph[t,k] x_t to the
+//     accumulators, so accumulator read-modify-write traffic drops by R.
+//   * One chunk of R steps (R/TB step launches + fold + counter advance) is
 //     captured once as a CUDA graph and replayed; kernels read the absolute
 //     step index from a device counter.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <mutex>
 
 #include "common.cuh"
@@ -40,31 +44,52 @@
 namespace gdn {
 namespace tm2d {
 
-constexpr int TI = 16;    // tile rows (x, slow axis)
-constexpr int TJ = 64;    // tile columns (y, contiguous axis)
-constexpr int HALO = 4;   // column halo in shared memory (16 B of f32)
-constexpr int PADJ = 32;  // ghost columns on each side of a plane
-constexpr int NT = 256;   // threads per CTA
-constexpr int EW = TJ + 2 * HALO;
-constexpr int KMAX = 16;
+constexpr int PADJ = 32;  // ghost columns on each side of a plane (>= HJ)
+constexpr int PADI = 8;   // ghost rows above and below a plane (>= TB)
+constexpr int HJ = 4;     // column halo in shared memory (16 bytes of f32)
+constexpr int KMAX = 16;  // most DFT frequencies per run
+constexpr int MAXP = 64;  // most port records in one tile
+
+// Tile configurations (TB sub-steps, TI x TJ owned cells, NT threads).
+struct Cfg {
+  int tb, ti, tj, nt;
+};
+// Per field type three TB=4 shapes, largest first (pick_cfg chooses one from
+// the grid size; GDN_TM_TILE=0/1/2 forces one, for tuning). The one-step shape serves runs that record the energy every step.
+constexpr Cfg kCfgF32[3] = {{4, 64, 64, 512}, {4, 32, 64, 256}, {4, 16, 32, 128}};
+constexpr Cfg kCfgF64[3] = {{4, 28, 64, 512}, {4, 16, 64, 256}, {4, 16, 32, 128}};
+constexpr Cfg kCfgStep{1, 16, 64, 256};  // one step per launch (energy records)
 
 struct Pt {
-  int m, i, j, pad;  // point index, cell (i, j)
+  int m, i, j, owner;  // point index, cell, 1 if this tile owns the cell
+};
+
+// A DFT monitor resolved against the grid: box [lo0, lo0+h) x [lo1, lo1+w)
+// of component comp, stored at `off` in every monitor-ring slot.
+struct MonD {
+  int comp, lo0, lo1, h, w, pad;
+  long long count, off;
+  void* out;
 };
 
 template <typename T>
 struct Dev {
-  int nx, ny, ld, npml, R, n_steps, n_freq;
-  long long plane, slot;  // elements per plane and per ring slot (3 planes)
-  T* ring;
-  const T *ca, *cb, *eps;  // ca/cb: padded planes; eps: caller (nx, ny)
+  int nx, ny, ld, npml, n_steps, n_freq, R, tiles_x;
+  long long plane;    // elements per padded plane
+  T* state[2];        // ping-pong field slots, 3 planes each (ez, hx, hy)
+  T* mring;           // monitor ring: R slots x mon_cells
+  long long mon_cells;
+  int n_mons;
+  const MonD* mons;
+  const T *ca, *cb, *eps;  // ca/cb padded planes; eps caller (nx, ny)
   const T *ikx_e, *iky_e, *ikx_h, *iky_h;
   const T *b_ezx_lo, *c_ezx_lo, *b_ezx_hi, *c_ezx_hi;
   const T *b_ezy_lo, *c_ezy_lo, *b_ezy_hi, *c_ezy_hi;
   const T *b_hyx_lo, *c_hyx_lo, *b_hyx_hi, *c_hyx_hi;
   const T *b_hxy_lo, *c_hxy_lo, *b_hxy_hi, *c_hxy_hi;
-  T *ezx_lo, *ezx_hi, *ezy_lo, *ezy_hi;
-  T *hyx_lo[2], *hyx_hi[2], *hxy_lo[2], *hxy_hi[2];
+  // CPML psi as padded planes (zero outside the slabs), by launch parity:
+  // 4 consecutive planes ezx, ezy, hyx, hxy per parity.
+  T* psi[2];
   T dt_mu, inv_dx, inv_dy, dx, dy, dz;
   int n_src, n_ports, n_mx, n_my, n_probes;
   const int *src_off, *port_off, *mx_off, *my_off, *probe_off;
@@ -77,16 +102,9 @@ struct Dev {
   const int* step_base;
 };
 
-// Device copy of one DFT monitor (GdnDftMonitor resolved against the grid).
-struct Mon {
-  int comp, lo0, lo1, w;
-  long long count;
-  void* out;
-};
-
 // Offset of field cell (i, j) in a padded plane.
-__device__ __forceinline__ long long cell_at(int ld, int i, int j) {
-  return (long long)(i + 1) * ld + (j + PADJ);
+__device__ __host__ __forceinline__ long long cell_at(int ld, int i, int j) {
+  return (long long)(i + PADI) * ld + (j + PADJ);
 }
 
 __device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
@@ -112,216 +130,345 @@ __device__ __forceinline__ T point_value(const Dev<T>& d, const T* cur, const do
   return T(d.cw_env[n] * s);
 }
 
-// One CPML psi recursion (cpml.py:120-158): psi' = b psi + c diff, returns
-// diff/kappa + psi'. `store` is false on halo cells owned by another CTA.
+// ---------------------------------------------------------------------------
+// Point work of one sub-step on the staged region (fdtd2d.py:419-451, 461).
+// ---------------------------------------------------------------------------
+struct TileLists {
+  int mb, me, yb, ye, sb, se, pb, pe, qb, qe;
+};
+
+template <typename T, int EW, int NT>
+__device__ __forceinline__ void apply_magnetic(const Dev<T>& d, const TileLists& L, T* sHx,
+                                               T* sHy, int ie, int je, int n, int tid) {
+  for (int q = L.mb + tid; q < L.me; q += NT) {
+    const Pt pt = d.mx_pts[q];
+    atomicAdd(&sHx[(pt.i - ie) * EW + (pt.j - je)],
+              -(d.dt_mu * point_value(d, d.mx_cur, d.mx_w, d.ph_h, d.n_mx, pt.m, n)));
+  }
+  for (int q = L.yb + tid; q < L.ye; q += NT) {
+    const Pt pt = d.my_pts[q];
+    atomicAdd(&sHy[(pt.i - ie) * EW + (pt.j - je)],
+              -(d.dt_mu * point_value(d, d.my_cur, d.my_w, d.ph_h, d.n_my, pt.m, n)));
+  }
+}
+
+// Per-row / per-column CPML coefficients and validity masks of a general
+// tile, so its sweeps are branch-free: outside the slabs b = c = 0 and
+// 1/kappa = 1, which reproduces the plain update exactly (psi stays 0).
+template <typename T, int EH, int EW>
+struct Coef {
+  T rb_h[EH], rc_h[EH], rk_h[EH], rb_e[EH], rc_e[EH], rk_e[EH];  // hyx, ezx (by row)
+  T cb_h[EW], cc_h[EW], ck_h[EW], cb_e[EW], cc_e[EW], ck_e[EW];  // hxy, ezy (by column)
+  unsigned char r_hx[EH], r_hy[EH], r_e[EH], c_hx[EW], c_hy[EW], c_e[EW];
+};
+
+template <typename T, int EH, int EW, int NT>
+__device__ void fill_coef(const Dev<T>& d, Coef<T, EH, EW>& k, int ie, int je, int tid) {
+  const int nx = d.nx, ny = d.ny, m = d.npml;
+  for (int r = tid; r < EH; r += NT) {
+    const int i = ie + r;
+    T b = 0, c = 0, kk = 1;
+    if (i >= 0 && i < nx - 1) {
+      if (i < m) {
+        b = d.b_hyx_lo[i]; c = d.c_hyx_lo[i]; kk = d.ikx_h[i];
+      } else if (i >= nx - 1 - m) {
+        b = d.b_hyx_hi[i - (nx - 1 - m)]; c = d.c_hyx_hi[i - (nx - 1 - m)]; kk = d.ikx_h[i];
+      }
+    }
+    k.rb_h[r] = b; k.rc_h[r] = c; k.rk_h[r] = kk;
+    const int a = i - 1, ni = nx - 2;
+    b = 0; c = 0; kk = 1;
+    if (a >= 0 && a < ni) {
+      if (a < m) {
+        b = d.b_ezx_lo[a]; c = d.c_ezx_lo[a]; kk = d.ikx_e[a];
+      } else if (a >= ni - m) {
+        b = d.b_ezx_hi[a - (ni - m)]; c = d.c_ezx_hi[a - (ni - m)]; kk = d.ikx_e[a];
+      }
+    }
+    k.rb_e[r] = b; k.rc_e[r] = c; k.rk_e[r] = kk;
+    k.r_hx[r] = i >= 0 && i < nx;
+    k.r_hy[r] = i >= 0 && i < nx - 1;
+    k.r_e[r] = i >= 1 && i <= nx - 2;
+  }
+  for (int cidx = tid; cidx < EW; cidx += NT) {
+    const int j = je + cidx;
+    T b = 0, c = 0, kk = 1;
+    if (j >= 0 && j < ny - 1) {
+      if (j < m) {
+        b = d.b_hxy_lo[j]; c = d.c_hxy_lo[j]; kk = d.iky_h[j];
+      } else if (j >= ny - 1 - m) {
+        b = d.b_hxy_hi[j - (ny - 1 - m)]; c = d.c_hxy_hi[j - (ny - 1 - m)]; kk = d.iky_h[j];
+      }
+    }
+    k.cb_h[cidx] = b; k.cc_h[cidx] = c; k.ck_h[cidx] = kk;
+    const int bb = j - 1, nj = ny - 2;
+    b = 0; c = 0; kk = 1;
+    if (bb >= 0 && bb < nj) {
+      if (bb < m) {
+        b = d.b_ezy_lo[bb]; c = d.c_ezy_lo[bb]; kk = d.iky_e[bb];
+      } else if (bb >= nj - m) {
+        b = d.b_ezy_hi[bb - (nj - m)]; c = d.c_ezy_hi[bb - (nj - m)]; kk = d.iky_e[bb];
+      }
+    }
+    k.cb_e[cidx] = b; k.cc_e[cidx] = c; k.ck_e[cidx] = kk;
+    k.c_hx[cidx] = j >= 0 && j < ny - 1;
+    k.c_hy[cidx] = j >= 0 && j < ny;
+    k.c_e[cidx] = j >= 1 && j <= ny - 2;
+  }
+}
+
 template <typename T>
-__device__ __forceinline__ T psi_term(T diff, T ikappa, T b, T c, const T* src, T* dst,
-                                      bool store) {
-  const T p = b * *src + c * diff;
-  if (store) *dst = p;
-  return diff * ikappa + p;
+__device__ __forceinline__ void ld16(T* dst, const T* src) {
+  *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<const uint4*>(src);
+}
+template <typename T>
+__device__ __forceinline__ void st16(T* dst, const T* src) {
+  *reinterpret_cast<uint4*>(dst) = *reinterpret_cast<const uint4*>(src);
 }
 
 // ---------------------------------------------------------------------------
-// Fused step: E^n -> H^{n+1/2} -> E^{n+1} on one tile, plus point work.
+// TB fused time steps on one tile + halo (fdtd2d.py:412-464 per sub-step).
+// GEN = true: tiles that touch the CPML slabs or the PEC ring; psi of the
+// extended region lives in shared memory and per-row/column coefficients and
+// masks make the sweeps branch-free. GEN = false: interior tiles, no psi and
+// no masks. Both sweep 16-byte vectors of cells along a row.
 // ---------------------------------------------------------------------------
-template <typename T>
-__global__ void __launch_bounds__(NT) tm_step(Dev<T> d, int sub) {
-  __shared__ __align__(16) T sEz[TI + 2][EW];  // rows i0-1..i0+TI, cols j0-HALO..
-  __shared__ __align__(16) T sHx[TI][EW];      // rows i0..i0+TI-1, cols j0-HALO..
-  __shared__ __align__(16) T sHy[TI + 1][TJ];  // rows i0-1..i0+TI-1, cols j0..
-  __shared__ __align__(16) T sE1[TI][TJ];      // new Ez of the tile
-
-  const int n = *d.step_base + sub;
-  const int par = n & 1;
-  const int nx = d.nx, ny = d.ny, ld = d.ld, npml = d.npml;
-  const int i0 = blockIdx.y * TI, j0 = blockIdx.x * TJ;
-  const int tid = threadIdx.x;
-  const T* ez0 = d.ring + (long long)(n % d.R) * d.slot;
-  const T* hx0 = ez0 + d.plane;
-  const T* hy0 = hx0 + d.plane;
-  T* ez1 = d.ring + (long long)((n + 1) % d.R) * d.slot;
-  T* hx1 = ez1 + d.plane;
-  T* hy1 = hx1 + d.plane;
-
-  // ---- stage the tile + halo (16-byte async copies) ----
+template <typename T, int TB, int TI, int TJ, int NT, bool GEN>
+__global__ void __launch_bounds__(NT) tm_tb(Dev<T> d, const int* tiles, int sub0, int nsub) {
+  constexpr int EH = TI + 2 * TB;  // extended rows
+  constexpr int EW = TJ + 2 * HJ;  // extended columns
+  constexpr int EC = EH * EW;
   constexpr int V = 16 / sizeof(T);
-  for (int q = tid; q < (TI + 2) * (EW / V); q += NT) {
-    const int r = q / (EW / V), c = (q - r * (EW / V)) * V;
-    cp_async16(&sEz[r][c], ez0 + cell_at(ld, i0 - 1 + r, j0 - HALO + c));
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  T* sEz = reinterpret_cast<T*>(smem_raw);
+  T* sHx = sEz + EC;
+  T* sHy = sHx + EC;
+  T* sCa = sHy + EC;
+  T* sCb = sCa + EC;
+  T* sPsi = sCb + EC;  // GEN only: ezx, ezy, hyx, hxy
+  __shared__ T sEb[MAXP];       // Ez^n at owned port records
+  __shared__ T sPv[MAXP * TB];  // cb_vs * Vs of the tile's port records per sub-step
+  __shared__ Coef<T, GEN ? EH : 1, GEN ? EW : 1> K;
+
+  const int n0 = *d.step_base + sub0;
+  const int par = (n0 / TB) & 1;
+  const int nx = d.nx, ny = d.ny, ld = d.ld, npml = d.npml;
+  const int tile = tiles[blockIdx.x];
+  const int ty = tile / d.tiles_x, tx = tile - ty * d.tiles_x;
+  const int i0 = ty * TI, j0 = tx * TJ;
+  const int ie = i0 - TB, je = j0 - HJ;  // global cell of extended (0, 0)
+  const int tid = threadIdx.x;
+  const T* src = d.state[par];
+  T* dst = d.state[par ^ 1];
+
+  // ---- stage the extended region (16-byte async copies) ----
+  constexpr int CW = EW / V;
+  for (int q = tid; q < EH * CW; q += NT) {
+    const int r = q / CW, c = (q - r * CW) * V;
+    const long long g = cell_at(ld, ie + r, je + c);
+    cp_async16(sEz + r * EW + c, src + g);
+    cp_async16(sHx + r * EW + c, src + d.plane + g);
+    cp_async16(sHy + r * EW + c, src + 2 * d.plane + g);
+    cp_async16(sCa + r * EW + c, d.ca + g);
+    cp_async16(sCb + r * EW + c, d.cb + g);
   }
-  for (int q = tid; q < TI * (EW / V); q += NT) {
-    const int r = q / (EW / V), c = (q - r * (EW / V)) * V;
-    cp_async16(&sHx[r][c], hx0 + cell_at(ld, i0 + r, j0 - HALO + c));
+  if constexpr (GEN) {
+    const T* gp = d.psi[par];
+    for (int q = tid; q < EH * CW; q += NT) {
+      const int r = q / CW, c = (q - r * CW) * V;
+      const long long g = cell_at(ld, ie + r, je + c);
+      for (int t = 0; t < 4; ++t) cp_async16(sPsi + t * EC + r * EW + c, gp + t * d.plane + g);
+    }
+    fill_coef<T, EH, EW, NT>(d, K, ie, je, tid);
   }
-  for (int q = tid; q < (TI + 1) * (TJ / V); q += NT) {
-    const int r = q / (TJ / V), c = (q - r * (TJ / V)) * V;
-    cp_async16(&sHy[r][c], hy0 + cell_at(ld, i0 - 1 + r, j0 + c));
+  TileLists tl;
+  tl.mb = d.mx_off[tile]; tl.me = d.mx_off[tile + 1];
+  tl.yb = d.my_off[tile]; tl.ye = d.my_off[tile + 1];
+  tl.sb = d.src_off[tile]; tl.se = d.src_off[tile + 1];
+  tl.pb = d.port_off[tile]; tl.pe = d.port_off[tile + 1];
+  tl.qb = d.probe_off[tile]; tl.qe = d.probe_off[tile + 1];
+  for (int q = tid; q < (tl.pe - tl.pb) * nsub; q += NT) {
+    const int k = q / nsub, s = q - k * nsub;
+    const int m = d.port_pts[tl.pb + k].m;
+    sPv[k * TB + s] = d.cb_vs[m] * d.port_vs[(long long)(n0 + s) * d.n_ports + m];
   }
   cp_async_wait_all();
   __syncthreads();
+  const T dt_mu = d.dt_mu, inv_dx = d.inv_dx, inv_dy = d.inv_dy;
 
-  // ---- H sweep (fdtd2d.py:416-428) on the tile + its halo row/column ----
-  const T* hxy_lo_r = d.hxy_lo[par];
-  const T* hxy_hi_r = d.hxy_hi[par];
-  T* hxy_lo_w = d.hxy_lo[par ^ 1];
-  T* hxy_hi_w = d.hxy_hi[par ^ 1];
-  for (int q = tid; q < TI * (TJ + 1); q += NT) {
-    const int r = q / (TJ + 1), cc = q - r * (TJ + 1) - 1;  // cc = -1 is the halo column
-    const int i = i0 + r, j = j0 + cc;
-    if (i < nx && j >= 0 && j < ny - 1) {
-      const T diff = (sEz[r + 1][HALO + cc + 1] - sEz[r + 1][HALO + cc]) * d.inv_dy;
-      T term = diff;
-      if (j < npml) {
-        const long long o = (long long)i * npml + j;
-        term = psi_term(diff, d.iky_h[j], d.b_hxy_lo[j], d.c_hxy_lo[j], hxy_lo_r + o,
-                        hxy_lo_w + o, cc >= 0);
-      } else if (j >= ny - 1 - npml) {
-        const int s = j - (ny - 1 - npml);
-        const long long o = (long long)i * npml + s;
-        term = psi_term(diff, d.iky_h[j], d.b_hxy_hi[s], d.c_hxy_hi[s], hxy_hi_r + o,
-                        hxy_hi_w + o, cc >= 0);
+  for (int s = 0; s < nsub; ++s) {
+    const int n = n0 + s;
+    // ---- H sweep (fdtd2d.py:416-428) over the extended region ----
+    // The last element's right neighbour and the last row's lower neighbour
+    // read past the row: garbage that, like every halo value, only reaches
+    // cells outside the owned tile within TB sub-steps.
+    for (int q = tid * V; q < EC; q += NT * V) {
+      T e[V + 1], el[V], hx[V], hy[V];
+      ld16(e, sEz + q);
+      e[V] = sEz[q + V];
+      ld16(el, sEz + q + EW);
+      ld16(hx, sHx + q);
+      ld16(hy, sHy + q);
+      if constexpr (GEN) {
+        const int r = q / EW, c = q - r * EW;
+        T pxy[V], pyx[V];
+        ld16(pxy, sPsi + 3 * EC + q);
+        ld16(pyx, sPsi + 2 * EC + q);
+        const T rb = K.rb_h[r], rc = K.rc_h[r], rk = K.rk_h[r];
+        const bool rhx = K.r_hx[r], rhy = K.r_hy[r];
+#pragma unroll
+        for (int k = 0; k < V; ++k) {
+          const T dy_ = (e[k + 1] - e[k]) * inv_dy;
+          pxy[k] = K.cb_h[c + k] * pxy[k] + K.cc_h[c + k] * dy_;
+          const T thx = dy_ * K.ck_h[c + k] + pxy[k];
+          if (rhx && K.c_hx[c + k]) hx[k] -= dt_mu * thx;
+          const T dx_ = (el[k] - e[k]) * inv_dx;
+          pyx[k] = rb * pyx[k] + rc * dx_;
+          const T thy = dx_ * rk + pyx[k];
+          if (rhy && K.c_hy[c + k]) hy[k] += dt_mu * thy;
+        }
+        st16(sPsi + 3 * EC + q, pxy);
+        st16(sPsi + 2 * EC + q, pyx);
+      } else {
+#pragma unroll
+        for (int k = 0; k < V; ++k) {
+          hx[k] -= dt_mu * ((e[k + 1] - e[k]) * inv_dy);
+          hy[k] += dt_mu * ((el[k] - e[k]) * inv_dx);
+        }
       }
-      sHx[r][HALO + cc] -= d.dt_mu * term;
+      st16(sHx + q, hx);
+      st16(sHy + q, hy);
     }
-  }
-  const T* hyx_lo_r = d.hyx_lo[par];
-  const T* hyx_hi_r = d.hyx_hi[par];
-  T* hyx_lo_w = d.hyx_lo[par ^ 1];
-  T* hyx_hi_w = d.hyx_hi[par ^ 1];
-  for (int q = tid; q < (TI + 1) * TJ; q += NT) {
-    const int r = q / TJ, c = q - r * TJ;  // r = 0 is the halo row i0-1
-    const int i = i0 - 1 + r, j = j0 + c;
-    if (i >= 0 && i < nx - 1 && j < ny) {
-      const T diff = (sEz[r + 1][HALO + c] - sEz[r][HALO + c]) * d.inv_dx;
-      T term = diff;
-      if (i < npml) {
-        const long long o = (long long)i * ny + j;
-        term = psi_term(diff, d.ikx_h[i], d.b_hyx_lo[i], d.c_hyx_lo[i], hyx_lo_r + o,
-                        hyx_lo_w + o, r > 0);
-      } else if (i >= nx - 1 - npml) {
-        const int s = i - (nx - 1 - npml);
-        const long long o = (long long)s * ny + j;
-        term = psi_term(diff, d.ikx_h[i], d.b_hyx_hi[s], d.c_hyx_hi[s], hyx_hi_r + o,
-                        hyx_hi_w + o, r > 0);
-      }
-      sHy[r][c] += d.dt_mu * term;
+    __syncthreads();
+    if (tl.mb < tl.me || tl.yb < tl.ye) {
+      apply_magnetic<T, EW, NT>(d, tl, sHx, sHy, ie, je, n, tid);
+      __syncthreads();
     }
-  }
-  __syncthreads();
-
-  // Magnetic currents on the tile and its halo: H -= (dt/mu) M (fdtd2d.py:419-428).
-  const int tile = blockIdx.y * gridDim.x + blockIdx.x;
-  {
-    const int mb = d.mx_off[tile], me = d.mx_off[tile + 1];
-    const int yb = d.my_off[tile], ye = d.my_off[tile + 1];
-    if (mb < me || yb < ye) {
-      for (int q = mb + tid; q < me; q += NT) {
-        const Pt pt = d.mx_pts[q];
-        atomicAdd(&sHx[pt.i - i0][HALO + pt.j - j0],
-                  -(d.dt_mu * point_value(d, d.mx_cur, d.mx_w, d.ph_h, d.n_mx, pt.m, n)));
-      }
-      for (int q = yb + tid; q < ye; q += NT) {
-        const Pt pt = d.my_pts[q];
-        atomicAdd(&sHy[pt.i - (i0 - 1)][pt.j - j0],
-                  -(d.dt_mu * point_value(d, d.my_cur, d.my_w, d.ph_h, d.n_my, pt.m, n)));
+    // Port current on H^{n+1/2} and the Ez^n snapshot (fdtd2d.py:430-436).
+    if (tl.pb < tl.pe) {
+      for (int q = tl.pb + tid; q < tl.pe; q += NT) {
+        const Pt pt = d.port_pts[q];
+        if (!pt.owner) continue;
+        const int l = (pt.i - ie) * EW + (pt.j - je);
+        sEb[q - tl.pb] = sEz[l];
+        d.out_i[(long long)n * d.n_ports + pt.m] =
+            (sHy[l] - sHy[l - EW]) * d.dy - (sHx[l] - sHx[l - 1]) * d.dx;
       }
       __syncthreads();
     }
-  }
-
-  // Owned H^{n+1/2} back to the ring (ghost cells carry their zeros).
-  for (int q = tid; q < TI * (TJ / V); q += NT) {
-    const int r = q / (TJ / V), c = (q - r * (TJ / V)) * V;
-    *reinterpret_cast<uint4*>(hx1 + cell_at(ld, i0 + r, j0 + c)) =
-        *reinterpret_cast<const uint4*>(&sHx[r][HALO + c]);
-    *reinterpret_cast<uint4*>(hy1 + cell_at(ld, i0 + r, j0 + c)) =
-        *reinterpret_cast<const uint4*>(&sHy[r + 1][c]);
-  }
-
-  // ---- E sweep on the interior (fdtd2d.py:438-443) ----
-  const int nxi = nx - 2, nyi = ny - 2;
-  for (int q = tid; q < TI * TJ; q += NT) {
-    const int r = q / TJ, c = q - r * TJ;
-    const int i = i0 + r, j = j0 + c;
-    T e1 = sEz[r + 1][HALO + c];
-    if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2) {
-      const T dhy_dx = (sHy[r + 1][c] - sHy[r][c]) * d.inv_dx;
-      const T dhx_dy = (sHx[r][HALO + c] - sHx[r][HALO + c - 1]) * d.inv_dy;
-      T tx = dhy_dx, ty = dhx_dy;
-      const int a = i - 1, b = j - 1;
-      if (a < npml) {
-        T* ps = d.ezx_lo + (long long)a * nyi + b;
-        tx = psi_term(dhy_dx, d.ikx_e[a], d.b_ezx_lo[a], d.c_ezx_lo[a], ps, ps, true);
-      } else if (a >= nxi - npml) {
-        const int s = a - (nxi - npml);
-        T* ps = d.ezx_hi + (long long)s * nyi + b;
-        tx = psi_term(dhy_dx, d.ikx_e[a], d.b_ezx_hi[s], d.c_ezx_hi[s], ps, ps, true);
+    // ---- E sweep (fdtd2d.py:438-443), in place ----
+    for (int q = tid * V; q < EC; q += NT * V) {
+      T e[V], ca[V], cb[V], hx[V + 1], hy[V], hu[V];
+      ld16(e, sEz + q);
+      ld16(ca, sCa + q);
+      ld16(cb, sCb + q);
+      hx[0] = q > 0 ? sHx[q - 1] : T(0);
+      ld16(hx + 1, sHx + q);
+      ld16(hy, sHy + q);
+      ld16(hu, sHy + (q >= EW ? q - EW : q));
+      if constexpr (GEN) {
+        const int r = q / EW, c = q - r * EW;
+        T px[V], py[V];
+        ld16(px, sPsi + q);
+        ld16(py, sPsi + EC + q);
+        const T rb = K.rb_e[r], rc = K.rc_e[r], rk = K.rk_e[r];
+        const bool re = K.r_e[r];
+#pragma unroll
+        for (int k = 0; k < V; ++k) {
+          const T dhy_dx = (hy[k] - hu[k]) * inv_dx;
+          const T dhx_dy = (hx[k + 1] - hx[k]) * inv_dy;
+          px[k] = rb * px[k] + rc * dhy_dx;
+          py[k] = K.cb_e[c + k] * py[k] + K.cc_e[c + k] * dhx_dy;
+          const T tx_ = dhy_dx * rk + px[k];
+          const T ty_ = dhx_dy * K.ck_e[c + k] + py[k];
+          if (re && K.c_e[c + k]) e[k] = ca[k] * e[k] + cb[k] * (tx_ - ty_);
+        }
+        st16(sPsi + q, px);
+        st16(sPsi + EC + q, py);
+      } else {
+#pragma unroll
+        for (int k = 0; k < V; ++k)
+          e[k] = ca[k] * e[k] + cb[k] * ((hy[k] - hu[k]) * inv_dx - (hx[k + 1] - hx[k]) * inv_dy);
       }
-      if (b < npml) {
-        T* ps = d.ezy_lo + (long long)a * npml + b;
-        ty = psi_term(dhx_dy, d.iky_e[b], d.b_ezy_lo[b], d.c_ezy_lo[b], ps, ps, true);
-      } else if (b >= nyi - npml) {
-        const int s = b - (nyi - npml);
-        T* ps = d.ezy_hi + (long long)a * npml + s;
-        ty = psi_term(dhx_dy, d.iky_e[b], d.b_ezy_hi[s], d.c_ezy_hi[s], ps, ps, true);
-      }
-      const long long g = cell_at(ld, i, j);
-      e1 = d.ca[g] * e1 + d.cb[g] * (tx - ty);
-    }
-    sE1[r][c] = e1;
-  }
-
-  // ---- point work on the new Ez (fdtd2d.py:430-461) ----
-  const int sb = d.src_off[tile], se = d.src_off[tile + 1];
-  const int pb = d.port_off[tile], pe = d.port_off[tile + 1];
-  const int qb = d.probe_off[tile], qe = d.probe_off[tile + 1];
-  if (sb < se || pb < pe || qb < qe) {
-    __syncthreads();
-    // Jz line sources: Ez -= cb_src J (fdtd2d.py:444).
-    for (int q = sb + tid; q < se; q += NT) {
-      const Pt pt = d.src_pts[q];
-      atomicAdd(&sE1[pt.i - i0][pt.j - j0],
-                -(d.cb_src[pt.m] * point_value(d, d.src_cur, d.src_w, d.ph_e, d.n_src, pt.m, n)));
+      st16(sEz + q, e);
     }
     __syncthreads();
-    // RVS ports in port order: every injection first, then the V/I records.
-    if (tid == 0 && pb < pe) {
-      for (int q = pb; q < pe; ++q) {
-        const Pt pt = d.port_pts[q];
-        sE1[pt.i - i0][pt.j - j0] += -(d.cb_vs[pt.m] * d.port_vs[(long long)n * d.n_ports + pt.m]);
+    // Jz line sources on every copy: Ez -= cb_src J (fdtd2d.py:444).
+    if (tl.sb < tl.se) {
+      for (int q = tl.sb + tid; q < tl.se; q += NT) {
+        const Pt pt = d.src_pts[q];
+        atomicAdd(&sEz[(pt.i - ie) * EW + (pt.j - je)],
+                  -(d.cb_src[pt.m] * point_value(d, d.src_cur, d.src_w, d.ph_e, d.n_src, pt.m, n)));
       }
-      for (int q = pb; q < pe; ++q) {
-        const Pt pt = d.port_pts[q];
-        const int r = pt.i - i0, c = pt.j - j0;
-        const T cur = (sHy[r + 1][c] - sHy[r][c]) * d.dy -
-                      (sHx[r][HALO + c] - sHx[r][HALO + c - 1]) * d.dx;
-        d.out_i[(long long)n * d.n_ports + pt.m] = cur;
-        d.out_v[(long long)n * d.n_ports + pt.m] =
-            T(-0.5) * d.dz * (sEz[r + 1][HALO + c] + sE1[r][c]);
-      }
+      __syncthreads();
     }
-    __syncthreads();
-    for (int q = qb + tid; q < qe; q += NT) {
+    // RVS ports in port order: every injection, then V for owned records.
+    if (tl.pb < tl.pe) {
+      if (tid == 0) {
+        for (int q = tl.pb; q < tl.pe; ++q) {
+          const Pt pt = d.port_pts[q];
+          sEz[(pt.i - ie) * EW + (pt.j - je)] += -sPv[(q - tl.pb) * TB + s];
+        }
+        for (int q = tl.pb; q < tl.pe; ++q) {
+          const Pt pt = d.port_pts[q];
+          if (pt.owner)
+            d.out_v[(long long)n * d.n_ports + pt.m] =
+                T(-0.5) * d.dz * (sEb[q - tl.pb] + sEz[(pt.i - ie) * EW + (pt.j - je)]);
+        }
+      }
+      __syncthreads();
+    }
+    for (int q = tl.qb + tid; q < tl.qe; q += NT) {
       const Pt pt = d.probe_pts[q];
-      d.out_probe[(long long)n * d.n_probes + pt.m] = sE1[pt.i - i0][pt.j - j0];
+      d.out_probe[(long long)n * d.n_probes + pt.m] = sEz[(pt.i - ie) * EW + (pt.j - je)];
     }
+    // Monitored cells of the owned tile into ring slot n % R.
+    if (d.n_mons > 0) {
+      T* slot = d.mring + (long long)(n % d.R) * d.mon_cells;
+      for (int mm = 0; mm < d.n_mons; ++mm) {
+        const MonD mo = d.mons[mm];
+        const int a0 = max(mo.lo0, i0), a1 = min(mo.lo0 + mo.h, i0 + TI);
+        const int b0 = max(mo.lo1, j0), b1 = min(mo.lo1 + mo.w, j0 + TJ);
+        if (a0 >= a1 || b0 >= b1) continue;
+        const T* f = mo.comp == 0 ? sEz : (mo.comp == 1 ? sHx : sHy);
+        const int bw = b1 - b0;
+        for (int q = tid; q < (a1 - a0) * bw; q += NT) {
+          const int i = a0 + q / bw, j = b0 + q % bw;
+          slot[mo.off + (long long)(i - mo.lo0) * mo.w + (j - mo.lo1)] = f[(i - ie) * EW + (j - je)];
+        }
+      }
+    }
+    __syncthreads();
   }
-  __syncthreads();
-  for (int q = tid; q < TI * (TJ / V); q += NT) {
-    const int r = q / (TJ / V), c = (q - r * (TJ / V)) * V;
-    *reinterpret_cast<uint4*>(ez1 + cell_at(ld, i0 + r, j0 + c)) =
-        *reinterpret_cast<const uint4*>(&sE1[r][c]);
+
+  // ---- owned fields to the other state slot; owned psi back to the slabs ----
+  constexpr int TV = TJ / V;
+  for (int q = tid; q < TI * TV; q += NT) {
+    const int r = q / TV, c = (q - r * TV) * V;
+    const long long g = cell_at(ld, i0 + r, j0 + c);
+    const int l = (r + TB) * EW + (c + HJ);
+    st16(dst + g, sEz + l);
+    st16(dst + d.plane + g, sHx + l);
+    st16(dst + 2 * d.plane + g, sHy + l);
+  }
+  if constexpr (GEN) {
+    T* gp = d.psi[par ^ 1];
+    for (int q = tid; q < TI * TV; q += NT) {
+      const int r = q / TV, c = (q - r * TV) * V;
+      const long long g = cell_at(ld, i0 + r, j0 + c);
+      const int l = (r + TB) * EW + (c + HJ);
+      for (int t = 0; t < 4; ++t) st16(gp + t * d.plane + g, sPsi + t * EC + l);
+    }
   }
 }
 
 // ---------------------------------------------------------------------------
-// Running DFT fold over `cnt` ring snapshots (fdtd2d.py:453-458): for each
-// accumulated cell, acc_k += sum_t ph[n0+t, k] * x_t, partial sums in A.
+// Running DFT fold over `cnt` monitor-ring slots (fdtd2d.py:453-458): for
+// each monitored cell, acc_k += sum_t ph[n0+t, k] x_t, partial sums in A.
 // ---------------------------------------------------------------------------
-template <typename T, typename A>
-__global__ void __launch_bounds__(256) tm_dft_fold(Dev<T> d, const Mon* mons, int sub0, int cnt) {
-  extern __shared__ unsigned char smem_raw[];
+template <typename T, typename A, int KM>
+__global__ void __launch_bounds__(256) tm_dft_fold(Dev<T> d, int sub0, int cnt) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   A* sph = reinterpret_cast<A*>(smem_raw);  // [2 tables][cnt][K][re, im]
   using C = typename Cplx<A>::type;
   const int n0 = *d.step_base + sub0;
@@ -336,22 +483,19 @@ __global__ void __launch_bounds__(256) tm_dft_fold(Dev<T> d, const Mon* mons, in
     sph[2 * (cnt * K + idx) + 1] = A(ph.y);
   }
   __syncthreads();
-  const Mon mon = mons[blockIdx.y];
+  const MonD mon = d.mons[blockIdx.y];
   const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= mon.count) return;
-  const int ri = int(r / mon.w), rj = int(r - (long long)ri * mon.w);
   const A* ph = sph + (mon.comp == 0 ? 0 : 2 * cnt * K);
-  const long long field_off =
-      (long long)mon.comp * d.plane + cell_at(d.ld, mon.lo0 + ri, mon.lo1 + rj);
-  A are[KMAX], aim[KMAX];
+  A are[KM], aim[KM];
 #pragma unroll
-  for (int k = 0; k < KMAX; ++k) are[k] = aim[k] = A(0);
+  for (int k = 0; k < KM; ++k) are[k] = aim[k] = A(0);
+  const T* base = d.mring + mon.off + r;
 #pragma unroll 4
   for (int t = 0; t < cnt; ++t) {
-    const int slot = (n0 + t + 1) % d.R;
-    const A x = A(d.ring[(long long)slot * d.slot + field_off]);
+    const A x = A(base[(long long)((n0 + t) % d.R) * d.mon_cells]);
 #pragma unroll
-    for (int k = 0; k < KMAX; ++k) {
+    for (int k = 0; k < KM; ++k) {
       if (k < K) {
         are[k] += ph[2 * (t * K + k)] * x;
         aim[k] += ph[2 * (t * K + k) + 1] * x;
@@ -360,7 +504,7 @@ __global__ void __launch_bounds__(256) tm_dft_fold(Dev<T> d, const Mon* mons, in
   }
   C* acc = static_cast<C*>(mon.out) + r;
 #pragma unroll
-  for (int k = 0; k < KMAX; ++k) {
+  for (int k = 0; k < KM; ++k) {
     if (k < K) {
       C v = acc[(long long)k * mon.count];
       v.x += are[k];
@@ -370,24 +514,22 @@ __global__ void __launch_bounds__(256) tm_dft_fold(Dev<T> d, const Mon* mons, in
   }
 }
 
-// Total field energy 1/2 (eps Ez^2 + mu0 H^2) dA (fdtd2d.py:160-169), reduced
-// in double into eacc[2n] (electric sum) and eacc[2n+1] (magnetic sum).
+// Total field energy 1/2 (eps Ez^2 + mu0 H^2) dA (fdtd2d.py:160-169) of the
+// state after step n, reduced in double into eacc[2n], eacc[2n+1].
 template <typename T>
 __global__ void tm_energy(Dev<T> d, double* eacc, int sub) {
   const int n = *d.step_base + sub;
-  const T* ez1 = d.ring + (long long)((n + 1) % d.R) * d.slot;
-  const T* hx1 = ez1 + d.plane;
-  const T* hy1 = hx1 + d.plane;
+  const T* f = d.state[(n + 1) & 1];  // one step per launch: state after step n
   double ue = 0.0, uh = 0.0;
   const long long total = (long long)d.nx * d.ny;
   for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
        g += (long long)gridDim.x * blockDim.x) {
     const int i = int(g / d.ny), j = int(g - (long long)i * d.ny);
     const long long c = cell_at(d.ld, i, j);
-    const double e = double(ez1[c]);
+    const double e = double(f[c]);
     ue += double(d.eps[g]) * e * e;
-    const double hx = double(hx1[c]), hy = double(hy1[c]);  // zero outside their grids
-    uh += hx * hx + hy * hy;
+    const double hx = double(f[d.plane + c]), hy = double(f[2 * d.plane + c]);
+    uh += hx * hx + hy * hy;  // zero outside their grids
   }
   for (int o = 16; o > 0; o >>= 1) {
     ue += __shfl_down_sync(0xffffffffu, ue, o);
@@ -435,7 +577,7 @@ __global__ void tm_pad_in(const T* src, T* dst, int nx, int ny, int ld) {
   }
 }
 
-// Copy the final ring slot into the caller's unpadded ez/hx/hy.
+// Copy the final state slot into the caller's unpadded ez/hx/hy.
 template <typename T>
 __global__ void tm_copy_out(const T* slot, long long plane, int nx, int ny, int ld, T* ez, T* hx,
                             T* hy) {
@@ -465,75 +607,128 @@ __global__ void tm_dft_scale(C* a, long long count, double s) {
 // Host side
 // ---------------------------------------------------------------------------
 
-
 struct Layout {
-  int ld = 0, rows = 0, R = 2, T = 32, tiles_x = 0, tiles_y = 0, n_tiles = 0;
-  long long plane = 0, slot = 0;
-  size_t ring, ca, cb, psi_e[4], psi_h[8], psi_end, off[5], pts[5], mons, step, eacc, total;
+  Cfg cfg;
+  int ld = 0, rows = 0, tiles_x = 0, tiles_y = 0, n_tiles = 0, R = 32, n_gen = 0, n_int = 0;
+  long long plane = 0, mon_cells = 0;
+  size_t state[2], ca, cb, psi[2], zero_end, tile_list, off[5], pts[5], mons, mring, step,
+      eacc, total;
 };
 
-static int dft_block_steps(const GdnTmParams* p, size_t slot_bytes) {
-  if (p->n_freq <= 0) return 32;
-  const size_t budget = size_t(2) << 30;  // ring budget: 2 GiB
-  long long t = (long long)(budget / std::max<size_t>(slot_bytes, 1)) - 1;
-  t = std::min<long long>(32, std::max<long long>(2, t));
-  return int(t);
+// Tile shape: one step per launch when the energy is recorded, else the
+// largest TB=4 shape that still yields two CTAs per SM's worth of tiles.
+static Cfg pick_cfg(const GdnTmParams* p, size_t esize) {
+  if (p->record_energy) return kCfgStep;
+  const Cfg* c = esize == sizeof(float) ? kCfgF32 : kCfgF64;
+  const char* env = getenv("GDN_TM_TILE");
+  if (env && env[0] >= '0' && env[0] <= '2' && env[1] == 0) return c[env[0] - '0'];
+  // Measured on B200 (f32): 64x64 tiles win once they give every SM a tile
+  // (1024^2: 129 vs 119/125 Gcell-steps/s); below that the 16x32 tiles keep
+  // more SMs busy (512^2: 47 vs 34; 140^2: 5.1 vs 2.7).
+  const long long big = div_up(p->nx, c[0].ti) * div_up(p->ny, c[0].tj);
+  return big >= 148 ? c[0] : c[2];
 }
 
-static Layout make_layout(const GdnTmParams* p, size_t esize) {
+static long long monitor_cells(const GdnTmParams* p, const GdnTmPoints* pts) {
+  if (p->n_freq <= 0) return 0;
+  if (p->n_monitors == 0)
+    return (long long)p->nx * p->ny + (long long)p->nx * (p->ny - 1) +
+           (long long)(p->nx - 1) * p->ny;
+  long long c = 0;
+  for (int k = 0; k < p->n_monitors; ++k) {
+    const GdnDftMonitor& m = pts->monitors[k];
+    c += (long long)(m.hi[0] - m.lo[0]) * (m.hi[1] - m.lo[1]);
+  }
+  return c;
+}
+
+// Interior tiles: every cell of the extended region is an interior Ez cell
+// outside all CPML slabs (x slabs are i <= npml or i >= nx-1-npml, likewise
+// y), so the interior kernel needs neither range checks nor psi. All other
+// tiles are "general".
+static bool tile_is_interior(const GdnTmParams* p, const Cfg& c, int ty, int tx) {
+  const int m = p->npml;
+  const int r0 = ty * c.ti - c.tb, r1 = (ty + 1) * c.ti + c.tb;
+  const int c0 = tx * c.tj - HJ, c1 = (tx + 1) * c.tj + HJ;
+  return r0 >= m + 1 && r1 - 1 <= p->nx - 2 - m && c0 >= m + 1 && c1 - 1 <= p->ny - 2 - m;
+}
+
+// `ring_steps` > 0 forces the monitor-ring length (a multiple of TB).
+static Layout make_layout(const GdnTmParams* p, const GdnTmPoints* pts, size_t esize,
+                          int ring_steps = 0) {
   Layout L;
-  L.tiles_x = int(div_up(p->ny, TJ));
-  L.tiles_y = int(div_up(p->nx, TI));
+  L.cfg = pick_cfg(p, esize);
+  const Cfg& c = L.cfg;
+  L.tiles_x = int(div_up(p->ny, c.tj));
+  L.tiles_y = int(div_up(p->nx, c.ti));
   L.n_tiles = L.tiles_x * L.tiles_y;
-  L.ld = PADJ + L.tiles_x * TJ + PADJ;
-  L.rows = L.tiles_y * TI + 2;
+  L.ld = PADJ + L.tiles_x * c.tj + PADJ;
+  L.rows = L.tiles_y * c.ti + 2 * PADI;
   L.plane = (long long)L.rows * L.ld;
-  L.slot = 3 * L.plane;
-  L.T = dft_block_steps(p, size_t(L.slot) * esize);
-  L.R = p->n_freq > 0 ? L.T + 1 : 2;
+  L.mon_cells = pts ? monitor_cells(p, pts) : 0;
+  if (ring_steps > 0) {
+    L.R = ring_steps;
+  } else {
+    const size_t budget = size_t(2) << 30;  // monitor ring budget: 2 GiB
+    long long r = L.mon_cells > 0 ? (long long)(budget / (size_t(L.mon_cells) * esize)) : 32;
+    r = std::min<long long>(32, r);
+    r = std::max<long long>(c.tb, r - r % c.tb);
+    L.R = int(r);
+  }
+  for (int ty = 0; ty < L.tiles_y; ++ty)
+    for (int tx = 0; tx < L.tiles_x; ++tx) {
+      if (tile_is_interior(p, c, ty, tx))
+        ++L.n_int;
+      else
+        ++L.n_gen;
+    }
   Carve cv;
-  L.ring = cv.take<char>(size_t(L.R) * L.slot * esize);
+  // Everything up to zero_end is cleared at the start of a run.
+  for (int s = 0; s < 2; ++s) L.state[s] = cv.take<char>(3 * size_t(L.plane) * esize);
   L.ca = cv.take<char>(size_t(L.plane) * esize);
   L.cb = cv.take<char>(size_t(L.plane) * esize);
-  const size_t m = size_t(p->npml), nx = size_t(p->nx), ny = size_t(p->ny);
-  const size_t pe[4] = {m * (ny - 2), m * (ny - 2), (nx - 2) * m, (nx - 2) * m};
-  for (int k = 0; k < 4; ++k) L.psi_e[k] = cv.take<char>(std::max<size_t>(pe[k], 1) * esize);
-  const size_t ph[4] = {m * ny, m * ny, nx * m, nx * m};  // hyx lo/hi, hxy lo/hi
-  for (int k = 0; k < 8; ++k) L.psi_h[k] = cv.take<char>(std::max<size_t>(ph[k / 2], 1) * esize);
-  L.psi_end = cv.take<char>(0);
+  for (int s = 0; s < 2; ++s) L.psi[s] = cv.take<char>(4 * size_t(L.plane) * esize);
+  L.step = cv.take<int>(1);
+  L.zero_end = cv.take<char>(0);
+  L.tile_list = cv.take<int>(L.n_tiles);  // general tiles first, then interior
   const int counts[5] = {p->n_sources, p->n_ports, p->n_mx, p->n_my, p->n_probes};
   for (int k = 0; k < 5; ++k) {
     L.off[k] = cv.take<int>(L.n_tiles + 1);
-    L.pts[k] = cv.take<Pt>(2 * size_t(std::max(counts[k], 1)));
+    L.pts[k] = cv.take<Pt>(4 * size_t(std::max(counts[k], 1)));
   }
-  L.mons = cv.take<Mon>(size_t(std::max(p->n_monitors, 3)));
-  L.step = cv.take<int>(1);
+  L.mons = cv.take<MonD>(size_t(std::max(p->n_monitors, 3)));
+  L.mring = cv.take<char>(std::max<size_t>(size_t(L.mon_cells) * L.R, 1) * esize);
   L.eacc = cv.take<double>(p->record_energy ? 2 * size_t(std::max(p->n_steps, 1)) : 1);
   L.total = cv.bytes();
   return L;
 }
 
-// Bin point records by the tiles that need them. kind 0: the owner tile of
-// an Ez cell; kind 1: Hx cells, also the right neighbour whose halo column
-// holds them; kind 2: Hy cells, also the lower neighbour whose halo row
-// holds them.
+// Bin point records by every tile whose extended region holds the cell;
+// `halo` = false keeps only the owner (probes). owner = 1 on the tile that
+// owns the cell.
 struct Bins {
   std::vector<int> off;
   std::vector<Pt> pts;
+  int max_per_tile = 0;
 };
 
-static Bins bin_tiles(int n, const int32_t* pi, const int32_t* pj, const Layout& L, int kind) {
+static Bins bin_tiles(int n, const int32_t* pi, const int32_t* pj, const Layout& L, bool halo) {
+  const Cfg& c = L.cfg;
   std::vector<std::pair<int, Pt>> rec;
-  rec.reserve(2 * size_t(n));
+  rec.reserve(4 * size_t(n));
   for (int m = 0; m < n; ++m) {
     const int i = pi[m], j = pj[m];
-    const int tx = j / TJ, ty = i / TI;
-    Pt pt{m, i, j, 0};
-    rec.push_back({ty * L.tiles_x + tx, pt});
-    if (kind == 1 && (j + 1) % TJ == 0 && tx + 1 < L.tiles_x)
-      rec.push_back({ty * L.tiles_x + tx + 1, pt});
-    if (kind == 2 && (i + 1) % TI == 0 && ty + 1 < L.tiles_y)
-      rec.push_back({(ty + 1) * L.tiles_x + tx, pt});
+    const int oty = i / c.ti, otx = j / c.tj;
+    for (int ty = std::max(0, oty - 1); ty <= std::min(L.tiles_y - 1, oty + 1); ++ty) {
+      for (int tx = std::max(0, otx - 1); tx <= std::min(L.tiles_x - 1, otx + 1); ++tx) {
+        const bool own = ty == oty && tx == otx;
+        if (!own && !halo) continue;
+        const int r0 = ty * c.ti - c.tb, r1 = (ty + 1) * c.ti + c.tb;
+        const int c0 = tx * c.tj - HJ, c1 = (tx + 1) * c.tj + HJ;
+        if (i < r0 || i >= r1 || j < c0 || j >= c1) continue;
+        rec.push_back({ty * L.tiles_x + tx, Pt{m, i, j, own ? 1 : 0}});
+      }
+    }
   }
   std::stable_sort(rec.begin(), rec.end(),
                    [](const std::pair<int, Pt>& a, const std::pair<int, Pt>& b) {
@@ -546,7 +741,10 @@ static Bins bin_tiles(int n, const int32_t* pi, const int32_t* pj, const Layout&
     b.off[rec[k].first + 1]++;
     b.pts[k] = rec[k].second;
   }
-  for (int t = 0; t < L.n_tiles; ++t) b.off[t + 1] += b.off[t];
+  for (int t = 0; t < L.n_tiles; ++t) {
+    b.max_per_tile = std::max(b.max_per_tile, b.off[t + 1]);
+    b.off[t + 1] += b.off[t];
+  }
   return b;
 }
 
@@ -627,42 +825,172 @@ static int validate(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuf
   return GDN_OK;
 }
 
+// Everything one run needs on the device, filled by prepare().
+template <typename T>
+struct Run {
+  Layout L;
+  Dev<T> d{};
+  std::vector<MonD> mons;
+  long long max_cells = 0;
+  double* eacc = nullptr;
+  int* step_base = nullptr;
+  const int* tiles = nullptr;  // L.n_gen general tile ids, then L.n_int interior
+};
+
+template <typename T, int TB, int TI, int TJ, bool GEN>
+static size_t tb_smem() {
+  return size_t(GEN ? 9 : 5) * (TI + 2 * TB) * (TJ + 2 * HJ) * sizeof(T);
+}
+
+// Per-type tile configurations: TB-step kernel and one-step kernel.
+template <typename T>
+struct Kern;
+template <>
+struct Kern<float> {
+  static constexpr Cfg c0 = kCfgF32[0], c1 = kCfgF32[1], c2 = kCfgF32[2];
+};
+template <>
+struct Kern<double> {
+  static constexpr Cfg c0 = kCfgF64[0], c1 = kCfgF64[1], c2 = kCfgF64[2];
+};
+
+template <typename T, int TB, int TI, int TJ, int NT, bool GEN>
+static int set_attr() {
+  GDN_TRY_CUDA(cudaFuncSetAttribute(tm_tb<T, TB, TI, TJ, NT, GEN>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    int(tb_smem<T, TB, TI, TJ, GEN>())));
+  return GDN_OK;
+}
 
 template <typename T>
-static int run(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuffers* b,
-               cudaStream_t stream) {
-  int st = validate(p, pts, b);
-  if (st) return st;
-  const Layout L = make_layout(p, sizeof(T));
-  char* ws = static_cast<char*>(b->workspace);
-  bool own = false;
-  if (!ws) {
-    GDN_TRY_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&ws), L.total, stream));
-    own = true;
-  } else if (b->workspace_bytes < L.total) {
-    GDN_BAD_ARG("workspace too small: %zu < %zu bytes", b->workspace_bytes, L.total);
-  }
-  struct Guard {
-    char* p;
-    bool own;
-    cudaStream_t s;
-    ~Guard() {
-      if (own && p) cudaFreeAsync(p, s);
-    }
-  } guard{ws, own, stream};
+static int set_kernel_attributes() {
+  static bool done = false;  // per process; the attribute is per function
+  if (done) return GDN_OK;
+  int st;
+  constexpr Cfg A = Kern<T>::c0, B = Kern<T>::c1, C = Kern<T>::c2, S = kCfgStep;
+  if ((st = set_attr<T, A.tb, A.ti, A.tj, A.nt, true>())) return st;
+  if ((st = set_attr<T, A.tb, A.ti, A.tj, A.nt, false>())) return st;
+  if ((st = set_attr<T, B.tb, B.ti, B.tj, B.nt, true>())) return st;
+  if ((st = set_attr<T, B.tb, B.ti, B.tj, B.nt, false>())) return st;
+  if ((st = set_attr<T, C.tb, C.ti, C.tj, C.nt, true>())) return st;
+  if ((st = set_attr<T, C.tb, C.ti, C.tj, C.nt, false>())) return st;
+  if ((st = set_attr<T, S.tb, S.ti, S.tj, S.nt, true>())) return st;
+  if ((st = set_attr<T, S.tb, S.ti, S.tj, S.nt, false>())) return st;
+  done = true;
+  return GDN_OK;
+}
 
+template <typename T, int TB, int TI, int TJ, int NT, bool GEN>
+static void launch_cfg(const Run<T>& R, const int* tiles, int count, int sub0, int nsub,
+                       cudaStream_t s) {
+  tm_tb<T, TB, TI, TJ, NT, GEN>
+      <<<count, NT, tb_smem<T, TB, TI, TJ, GEN>(), s>>>(R.d, tiles, sub0, nsub);
+}
+
+// Launch the general and the interior tiles for `nsub` steps starting at
+// chunk offset `sub0`; with a side stream the two run concurrently.
+template <typename T>
+static uint64_t launch_tb(const Run<T>& R, int sub0, int nsub, cudaStream_t s, cudaStream_t side,
+                          cudaEvent_t fork, cudaEvent_t join) {
+  constexpr Cfg A = Kern<T>::c0, B = Kern<T>::c1, C = Kern<T>::c2, S = kCfgStep;
+  const Cfg& c = R.L.cfg;
+  const int which = c.tb == 1 ? 3 : (c.ti == A.ti && c.tj == A.tj ? 0 : (c.ti == B.ti && c.tj == B.tj ? 1 : 2));
+  const int ng = R.L.n_gen, ni = R.L.n_int;
+  cudaStream_t si = s;
+  if (side && ng > 0 && ni > 0) {
+    cudaEventRecord(fork, s);
+    cudaStreamWaitEvent(side, fork, 0);
+    si = side;
+  }
+  uint64_t k = 0;
+#define GDN_LAUNCH(CF, GEN, TL, CNT, ST) \
+  launch_cfg<T, CF.tb, CF.ti, CF.tj, CF.nt, GEN>(R, TL, CNT, sub0, nsub, ST)
+  if (ng > 0) {
+    switch (which) {
+      case 0: GDN_LAUNCH(A, true, R.tiles, ng, s); break;
+      case 1: GDN_LAUNCH(B, true, R.tiles, ng, s); break;
+      case 2: GDN_LAUNCH(C, true, R.tiles, ng, s); break;
+      default: GDN_LAUNCH(S, true, R.tiles, ng, s); break;
+    }
+    ++k;
+  }
+  if (ni > 0) {
+    switch (which) {
+      case 0: GDN_LAUNCH(A, false, R.tiles + ng, ni, si); break;
+      case 1: GDN_LAUNCH(B, false, R.tiles + ng, ni, si); break;
+      case 2: GDN_LAUNCH(C, false, R.tiles + ng, ni, si); break;
+      default: GDN_LAUNCH(S, false, R.tiles + ng, ni, si); break;
+    }
+    ++k;
+  }
+#undef GDN_LAUNCH
+  if (si != s) {
+    cudaEventRecord(join, side);
+    cudaStreamWaitEvent(s, join, 0);
+  }
+  return k;
+}
+
+template <typename T, typename A>
+static void launch_fold(const Run<T>& R, int cnt, int K, cudaStream_t s) {
+  const dim3 dg(unsigned(div_up(R.max_cells, 256)), unsigned(R.mons.size()));
+  const size_t sm = size_t(4) * cnt * K * sizeof(A);
+  if (K <= 4)
+    tm_dft_fold<T, A, 4><<<dg, 256, sm, s>>>(R.d, 0, cnt);
+  else if (K <= 8)
+    tm_dft_fold<T, A, 8><<<dg, 256, sm, s>>>(R.d, 0, cnt);
+  else
+    tm_dft_fold<T, A, KMAX><<<dg, 256, sm, s>>>(R.d, 0, cnt);
+}
+
+// Enqueue one chunk of `cnt` steps (cnt <= R.L.R): step launches (+ energy),
+// the DFT fold and the counter advance. Returns the number of kernels.
+template <typename T>
+static uint64_t enqueue_chunk(const Run<T>& R, const GdnTmParams* p, int cnt, cudaStream_t s,
+                              cudaStream_t side = nullptr, cudaEvent_t fork = nullptr,
+                              cudaEvent_t join = nullptr) {
+  uint64_t k = 0;
+  const int tb = R.L.cfg.tb;
+  const int eblocks = int(std::min<long long>(div_up((long long)p->nx * p->ny, 256), 148 * 8));
+  for (int sub = 0; sub < cnt; sub += tb) {
+    k += launch_tb(R, sub, std::min(tb, cnt - sub), s, side, fork, join);
+    if (p->record_energy) {  // tb == 1 here
+      tm_energy<T><<<eblocks, 256, 0, s>>>(R.d, R.eacc, sub);
+      ++k;
+    }
+  }
+  if (!R.mons.empty()) {
+    if (p->dft_f64)
+      launch_fold<T, double>(R, cnt, p->n_freq, s);
+    else
+      launch_fold<T, float>(R, cnt, p->n_freq, s);
+    ++k;
+  }
+  tm_advance<<<1, 1, 0, s>>>(R.step_base, cnt);
+  return k + 1;
+}
+
+// Fill the device description, upload point bins and monitors, clear the
+// state that starts at zero and pad ca/cb in. `ws` holds L.total bytes.
+template <typename T>
+static int prepare(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuffers* b, char* ws,
+                   Run<T>& R, cudaStream_t stream) {
+  const Layout& L = R.L;
   const int nx = p->nx, ny = p->ny, N = p->n_steps;
-  Dev<T> d{};
+  Dev<T>& d = R.d;
   d.nx = nx;
   d.ny = ny;
   d.ld = L.ld;
   d.npml = p->npml;
-  d.R = L.R;
   d.n_steps = N;
   d.n_freq = p->n_freq;
+  d.R = L.R;
+  d.tiles_x = L.tiles_x;
   d.plane = L.plane;
-  d.slot = L.slot;
-  d.ring = reinterpret_cast<T*>(ws + L.ring);
+  d.state[0] = reinterpret_cast<T*>(ws + L.state[0]);
+  d.state[1] = reinterpret_cast<T*>(ws + L.state[1]);
+  d.mring = reinterpret_cast<T*>(ws + L.mring);
+  d.mon_cells = L.mon_cells;
   d.ca = reinterpret_cast<const T*>(ws + L.ca);
   d.cb = reinterpret_cast<const T*>(ws + L.cb);
   d.eps = static_cast<const T*>(b->eps);
@@ -676,16 +1004,7 @@ static int run(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuffers*
   GDN_TAB(b_hyx_lo); GDN_TAB(c_hyx_lo); GDN_TAB(b_hyx_hi); GDN_TAB(c_hyx_hi);
   GDN_TAB(b_hxy_lo); GDN_TAB(c_hxy_lo); GDN_TAB(b_hxy_hi); GDN_TAB(c_hxy_hi);
 #undef GDN_TAB
-  d.ezx_lo = reinterpret_cast<T*>(ws + L.psi_e[0]);
-  d.ezx_hi = reinterpret_cast<T*>(ws + L.psi_e[1]);
-  d.ezy_lo = reinterpret_cast<T*>(ws + L.psi_e[2]);
-  d.ezy_hi = reinterpret_cast<T*>(ws + L.psi_e[3]);
-  for (int par = 0; par < 2; ++par) {
-    d.hyx_lo[par] = reinterpret_cast<T*>(ws + L.psi_h[0 + par]);
-    d.hyx_hi[par] = reinterpret_cast<T*>(ws + L.psi_h[2 + par]);
-    d.hxy_lo[par] = reinterpret_cast<T*>(ws + L.psi_h[4 + par]);
-    d.hxy_hi[par] = reinterpret_cast<T*>(ws + L.psi_h[6 + par]);
-  }
+  for (int s = 0; s < 2; ++s) d.psi[s] = reinterpret_cast<T*>(ws + L.psi[s]);
   d.dt_mu = T(b->dt_mu);
   d.inv_dx = T(b->inv_dx);
   d.inv_dy = T(b->inv_dy);
@@ -713,19 +1032,21 @@ static int run(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuffers*
   d.out_probe = static_cast<T*>(b->out_probe);
   d.out_v = static_cast<T*>(b->out_v);
   d.out_i = static_cast<T*>(b->out_i);
-  int* step_base = reinterpret_cast<int*>(ws + L.step);
-  d.step_base = step_base;
+  R.step_base = reinterpret_cast<int*>(ws + L.step);
+  d.step_base = R.step_base;
+  R.eacc = reinterpret_cast<double*>(ws + L.eacc);
 
-  // Bin the point lists by tile and upload them (pageable copies are staged
-  // before cudaMemcpyAsync returns, so the host vectors may go out of scope).
+  // Point bins (with halo copies except for probes). Pageable copies are
+  // staged before cudaMemcpyAsync returns, so the vectors may go away.
   const int counts[5] = {p->n_sources, p->n_ports, p->n_mx, p->n_my, p->n_probes};
   const int32_t* is[5] = {pts->src_i, pts->port_i, pts->mx_i, pts->my_i, pts->probe_i};
   const int32_t* js[5] = {pts->src_j, pts->port_j, pts->mx_j, pts->my_j, pts->probe_j};
-  const int kinds[5] = {0, 0, 1, 2, 0};
   const int* offs[5];
   const Pt* pls[5];
   for (int k = 0; k < 5; ++k) {
-    Bins bn = bin_tiles(counts[k], is[k], js[k], L, kinds[k]);
+    Bins bn = bin_tiles(counts[k], is[k], js[k], L, k != 4);
+    if (k == 1 && bn.max_per_tile > MAXP)
+      GDN_BAD_ARG("%d port records fall in one tile (at most %d)", bn.max_per_tile, MAXP);
     GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.off[k], bn.off.data(), bn.off.size() * sizeof(int),
                                  cudaMemcpyHostToDevice, stream));
     if (!bn.pts.empty())
@@ -740,68 +1061,139 @@ static int run(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuffers*
   d.my_off = offs[3]; d.my_pts = pls[3];
   d.probe_off = offs[4]; d.probe_pts = pls[4];
 
-  // Zero the state (ring, padded ca/cb, psi, counter, energy) and pad ca/cb in.
-  GDN_TRY_CUDA(cudaMemsetAsync(ws + L.ring, 0, L.psi_end - L.ring, stream));
-  GDN_TRY_CUDA(cudaMemsetAsync(step_base, 0, sizeof(int), stream));
+  // Tile lists: general tiles first, then interior tiles.
+  {
+    std::vector<int> gen, inr;
+    for (int ty = 0; ty < L.tiles_y; ++ty)
+      for (int tx = 0; tx < L.tiles_x; ++tx)
+        (tile_is_interior(p, L.cfg, ty, tx) ? inr : gen).push_back(ty * L.tiles_x + tx);
+    gen.insert(gen.end(), inr.begin(), inr.end());
+    GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.tile_list, gen.data(), gen.size() * sizeof(int),
+                                 cudaMemcpyHostToDevice, stream));
+    R.tiles = reinterpret_cast<const int*>(ws + L.tile_list);
+  }
+
+  // Monitors (full grid when none are listed).
+  const bool f64acc = p->dft_f64 != 0;
+  const size_t csz = f64acc ? sizeof(double2) : sizeof(float2);
+  R.mons.clear();
+  if (p->n_freq > 0) {
+    long long off = 0;
+    if (p->n_monitors == 0) {
+      void* const outs[3] = {b->dft_ez, b->dft_hx, b->dft_hy};
+      const int shp[3][2] = {{nx, ny}, {nx, ny - 1}, {nx - 1, ny}};
+      for (int c = 0; c < 3; ++c) {
+        const long long cnt = (long long)shp[c][0] * shp[c][1];
+        R.mons.push_back(MonD{c, 0, 0, shp[c][0], shp[c][1], 0, cnt, off, outs[c]});
+        off += cnt;
+      }
+    } else {
+      for (int k = 0; k < p->n_monitors; ++k) {
+        const GdnDftMonitor& m = pts->monitors[k];
+        const int h = m.hi[0] - m.lo[0], w = m.hi[1] - m.lo[1];
+        R.mons.push_back(MonD{m.comp, m.lo[0], m.lo[1], h, w, 0, (long long)h * w, off, m.out});
+        off += (long long)h * w;
+      }
+    }
+  }
+  d.n_mons = int(R.mons.size());
+  d.mons = reinterpret_cast<const MonD*>(ws + L.mons);
+  R.max_cells = 0;
+  for (const MonD& m : R.mons) {
+    R.max_cells = std::max(R.max_cells, m.count);
+    GDN_TRY_CUDA(cudaMemsetAsync(m.out, 0, size_t(m.count) * p->n_freq * csz, stream));
+  }
+  if (!R.mons.empty())
+    GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.mons, R.mons.data(), R.mons.size() * sizeof(MonD),
+                                 cudaMemcpyHostToDevice, stream));
+
+  // Clear the state that starts at zero: both field slots (ghost cells
+  // included), padded ca/cb, both psi parities, the step counter.
+  GDN_TRY_CUDA(cudaMemsetAsync(ws + L.state[0], 0, L.zero_end - L.state[0], stream));
+  if (p->record_energy)
+    GDN_TRY_CUDA(cudaMemsetAsync(R.eacc, 0, 2 * size_t(std::max(N, 1)) * sizeof(double), stream));
   const int eblocks = int(std::min<long long>(div_up((long long)nx * ny, 256), 148 * 8));
   tm_pad_in<T><<<eblocks, 256, 0, stream>>>(static_cast<const T*>(b->ca),
                                              reinterpret_cast<T*>(ws + L.ca), nx, ny, L.ld);
   tm_pad_in<T><<<eblocks, 256, 0, stream>>>(static_cast<const T*>(b->cb),
                                              reinterpret_cast<T*>(ws + L.cb), nx, ny, L.ld);
   count_launches(2);
-  double* eacc = reinterpret_cast<double*>(ws + L.eacc);
-  if (p->record_energy)
-    GDN_TRY_CUDA(cudaMemsetAsync(eacc, 0, 2 * size_t(std::max(N, 1)) * sizeof(double), stream));
+  return GDN_OK;
+}
 
-  const bool f64acc = p->dft_f64 != 0;
-  const size_t csz = f64acc ? sizeof(double2) : sizeof(float2);
-  std::vector<Mon> mons;
-  if (p->n_freq > 0) {
-    if (p->n_monitors == 0) {
-      void* const outs[3] = {b->dft_ez, b->dft_hx, b->dft_hy};
-      const int shp[3][2] = {{nx, ny}, {nx, ny - 1}, {nx - 1, ny}};
-      for (int c = 0; c < 3; ++c)
-        mons.push_back(Mon{c, 0, 0, shp[c][1], (long long)shp[c][0] * shp[c][1], outs[c]});
-    } else {
-      for (int k = 0; k < p->n_monitors; ++k) {
-        const GdnDftMonitor& m = pts->monitors[k];
-        const int h = m.hi[0] - m.lo[0], w = m.hi[1] - m.lo[1];
-        mons.push_back(Mon{m.comp, m.lo[0], m.lo[1], w, (long long)h * w, m.out});
-      }
+// Copy the final fields out, scale the DFT by dt (fdtd2d.py:482-487), finish
+// the energy record.
+template <typename T>
+static int finalize(const GdnTmParams* p, const GdnTmBuffers* b, const Run<T>& R,
+                    cudaStream_t stream) {
+  const int nx = p->nx, ny = p->ny, N = p->n_steps;
+  const long long launches = div_up(N, R.L.cfg.tb);
+  const T* last = R.d.state[launches & 1];
+  const int eblocks = int(std::min<long long>(div_up((long long)nx * ny, 256), 148 * 8));
+  tm_copy_out<T><<<eblocks, 256, 0, stream>>>(last, R.L.plane, nx, ny, R.L.ld,
+                                              static_cast<T*>(b->ez), static_cast<T*>(b->hx),
+                                              static_cast<T*>(b->hy));
+  for (const MonD& m : R.mons) {
+    const long long cnt = m.count * p->n_freq;
+    const int blocks = int(std::min<long long>(div_up(cnt, 256), 148 * 8));
+    if (p->dft_f64)
+      tm_dft_scale<double2><<<blocks, 256, 0, stream>>>(static_cast<double2*>(m.out), cnt, p->dt);
+    else
+      tm_dft_scale<float2><<<blocks, 256, 0, stream>>>(static_cast<float2*>(m.out), cnt, p->dt);
+  }
+  if (p->record_energy && N > 0)
+    tm_energy_finish<T><<<unsigned(div_up(N, 256)), 256, 0, stream>>>(
+        R.eacc, static_cast<T*>(b->out_energy), N, p->dx * p->dy, p->mu0);
+  count_launches(1 + R.mons.size() + (p->record_energy && N > 0 ? 1 : 0));
+  GDN_TRY_CUDA(cudaGetLastError());
+  return GDN_OK;
+}
+
+template <typename T>
+static int run(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuffers* b,
+               cudaStream_t stream) {
+  int st = validate(p, pts, b);
+  if (st) return st;
+  if ((st = set_kernel_attributes<T>())) return st;
+  Run<T> R;
+  R.L = make_layout(p, pts, sizeof(T));
+  char* ws = static_cast<char*>(b->workspace);
+  bool own = false;
+  if (!ws) {
+    GDN_TRY_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&ws), R.L.total, stream));
+    own = true;
+  } else if (b->workspace_bytes < R.L.total) {
+    GDN_BAD_ARG("workspace too small: %zu < %zu bytes", b->workspace_bytes, R.L.total);
+  }
+  struct Guard {
+    char* p;
+    bool own;
+    cudaStream_t s;
+    ~Guard() {
+      if (own && p) cudaFreeAsync(p, s);
     }
-  }
-  long long max_cells = 0;
-  for (const Mon& m : mons) {
-    max_cells = std::max(max_cells, m.count);
-    GDN_TRY_CUDA(cudaMemsetAsync(m.out, 0, size_t(m.count) * p->n_freq * csz, stream));
-  }
-  const Mon* d_mons = reinterpret_cast<const Mon*>(ws + L.mons);
-  if (!mons.empty())
-    GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.mons, mons.data(), mons.size() * sizeof(Mon),
-                                 cudaMemcpyHostToDevice, stream));
+  } guard{ws, own, stream};
+  if ((st = prepare(p, pts, b, ws, R, stream))) return st;
 
-  const dim3 grd(L.tiles_x, L.tiles_y);
-
-  // Capture one chunk of `cnt` steps as a graph.
+  // Capture one chunk of `cnt` steps as a graph; the general and interior
+  // tile launches of each block become parallel branches.
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  GDN_TRY_CUDA(cudaEventCreateWithFlags(&ev_fork, cudaEventDisableTiming));
+  GDN_TRY_CUDA(cudaEventCreateWithFlags(&ev_join, cudaEventDisableTiming));
+  struct EvGuard {
+    cudaEvent_t a, b;
+    ~EvGuard() {
+      cudaEventDestroy(a);
+      cudaEventDestroy(b);
+    }
+  } ev_guard{ev_fork, ev_join};
+  uint64_t per_chunk = 0;
   auto capture = [&](int cnt, cudaGraphExec_t* exec) -> int {
     cudaStream_t cs = capture_stream();
     if (!cs) GDN_BAD_ARG("no capture stream for this device");
+    cudaStream_t side = capture_side_stream();
     GDN_TRY_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-    for (int s = 0; s < cnt; ++s) {
-      tm_step<T><<<grd, NT, 0, cs>>>(d, s);
-      if (p->record_energy) tm_energy<T><<<eblocks, 256, 0, cs>>>(d, eacc, s);
-    }
-    if (!mons.empty()) {
-      const dim3 dg(unsigned(div_up(max_cells, 256)), unsigned(mons.size()));
-      if (f64acc) {
-        const size_t sm = size_t(4) * cnt * p->n_freq * sizeof(double);
-        tm_dft_fold<T, double><<<dg, 256, sm, cs>>>(d, d_mons, 0, cnt);
-      } else {
-        const size_t sm = size_t(4) * cnt * p->n_freq * sizeof(float);
-        tm_dft_fold<T, float><<<dg, 256, sm, cs>>>(d, d_mons, 0, cnt);
-      }
-    }
-    tm_advance<<<1, 1, 0, cs>>>(step_base, cnt);
+    per_chunk = enqueue_chunk(R, p, cnt, cs, side, ev_fork, ev_join);
     cudaGraph_t g = nullptr;
     const cudaError_t e1 = cudaStreamEndCapture(cs, &g);
     if (e1 != cudaSuccess) {
@@ -816,54 +1208,39 @@ static int run(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuffers*
     }
     return GDN_OK;
   };
-
-  const int Tc = L.T;
+  const int N = p->n_steps, Tc = R.L.R;
   const int full = N / Tc, rem = N % Tc;
   cudaGraphExec_t g_full = nullptr, g_rem = nullptr;
-  if (full > 0 && (st = capture(Tc, &g_full))) return st;
-  if (rem > 0 && (st = capture(rem, &g_rem))) {
-    if (g_full) cudaGraphExecDestroy(g_full);
-    return st;
+  uint64_t k_full = 0, k_rem = 0;
+  if (full > 0) {
+    if ((st = capture(Tc, &g_full))) return st;
+    k_full = per_chunk;
   }
-  // Kernel nodes per chunk graph: steps (+ energy), DFT fold, counter advance.
-  auto nodes = [&](int cnt) -> uint64_t {
-    return uint64_t(cnt) * (p->record_energy ? 2 : 1) + (mons.empty() ? 0 : 1) + 1;
-  };
+  if (rem > 0) {
+    if ((st = capture(rem, &g_rem))) {
+      if (g_full) cudaGraphExecDestroy(g_full);
+      return st;
+    }
+    k_rem = per_chunk;
+  }
   cudaError_t le = cudaSuccess;
   for (int c = 0; c < full && le == cudaSuccess; ++c) le = cudaGraphLaunch(g_full, stream);
   if (rem > 0 && le == cudaSuccess) le = cudaGraphLaunch(g_rem, stream);
-  count_launches(uint64_t(full) * (full ? nodes(Tc) : 0) + (rem ? nodes(rem) : 0));
   if (g_full) cudaGraphExecDestroy(g_full);
   if (g_rem) cudaGraphExecDestroy(g_rem);
   if (le != cudaSuccess) {
     set_error("graph launch failed: %s", cudaGetErrorString(le));
     return GDN_ERR_CUDA;
   }
-
-  // Finalise: fields out, DFT x dt (fdtd2d.py:482-487), energy.
-  const T* last = d.ring + (long long)(N % L.R) * L.slot;
-  tm_copy_out<T><<<eblocks, 256, 0, stream>>>(last, L.plane, nx, ny, L.ld, static_cast<T*>(b->ez),
-                                              static_cast<T*>(b->hx), static_cast<T*>(b->hy));
-  for (const Mon& m : mons) {
-    const long long cnt = m.count * p->n_freq;
-    const int blocks = int(std::min<long long>(div_up(cnt, 256), 148 * 8));
-    if (f64acc)
-      tm_dft_scale<double2><<<blocks, 256, 0, stream>>>(static_cast<double2*>(m.out), cnt, p->dt);
-    else
-      tm_dft_scale<float2><<<blocks, 256, 0, stream>>>(static_cast<float2*>(m.out), cnt, p->dt);
-  }
-  count_launches(1 + mons.size() + (p->record_energy && N > 0 ? 1 : 0));
-  if (p->record_energy && N > 0)
-    tm_energy_finish<T><<<unsigned(div_up(N, 256)), 256, 0, stream>>>(
-        eacc, static_cast<T*>(b->out_energy), N, p->dx * p->dy, p->mu0);
-  GDN_TRY_CUDA(cudaGetLastError());
-  return GDN_OK;
+  count_launches(uint64_t(full) * k_full + k_rem);
+  return finalize(p, b, R, stream);
 }
 
 }  // namespace tm2d
 }  // namespace gdn
 
-extern "C" int gdn_tm_workspace_size(const GdnTmParams* p, int f64, size_t* bytes) {
+extern "C" int gdn_tm_workspace_size(const GdnTmParams* p, const GdnTmPoints* pts, int f64,
+                                     size_t* bytes) {
   if (!p || !bytes) {
     gdn::set_error("null argument");
     return GDN_ERR_BAD_ARG;
@@ -872,7 +1249,11 @@ extern "C" int gdn_tm_workspace_size(const GdnTmParams* p, int f64, size_t* byte
     gdn::set_error("invalid grid");
     return GDN_ERR_BAD_ARG;
   }
-  *bytes = gdn::tm2d::make_layout(p, f64 ? sizeof(double) : sizeof(float)).total;
+  if (p->n_freq > 0 && p->n_monitors > 0 && (!pts || !pts->monitors)) {
+    gdn::set_error("monitor list is null");
+    return GDN_ERR_BAD_ARG;
+  }
+  *bytes = gdn::tm2d::make_layout(p, pts, f64 ? sizeof(double) : sizeof(float)).total;
   return GDN_OK;
 }
 
@@ -893,10 +1274,10 @@ extern "C" int gdn_tm_run_f64(const GdnTmParams* p, const GdnTmPoints* pts,
 // code that owns the GPU's memory through its own pool (the allocation would
 // fail or fragment that pool), real-time loops that forbid allocator calls,
 // and hosts that load this library without a CUDA allocator they may use.
-// The scratch (field ring, psi slabs, point bins, monitor table, step
-// counter) lives in one file-scope __device__ array of fixed size instead of
-// a workspace. Every GPU that loads this library holds the array until the
-// process exits.
+// The scratch (field state, psi slabs, point bins, monitor table and ring,
+// step counter) lives in one file-scope __device__ array of fixed size
+// instead of a workspace. Every GPU that loads this library holds the array
+// until the process exits.
 // ===========================================================================
 namespace gdn {
 namespace tm2d {
@@ -924,40 +1305,6 @@ static int static_scratch(char** out) {
   return GDN_OK;
 }
 
-// make_layout with an explicit DFT fold length T (the ring has T+1 slots).
-static Layout make_layout_fold(const GdnTmParams* p, size_t esize, int T) {
-  Layout L;
-  L.tiles_x = int(div_up(p->ny, TJ));
-  L.tiles_y = int(div_up(p->nx, TI));
-  L.n_tiles = L.tiles_x * L.tiles_y;
-  L.ld = PADJ + L.tiles_x * TJ + PADJ;
-  L.rows = L.tiles_y * TI + 2;
-  L.plane = (long long)L.rows * L.ld;
-  L.slot = 3 * L.plane;
-  L.T = T;
-  L.R = p->n_freq > 0 ? T + 1 : 2;
-  Carve cv;
-  L.ring = cv.take<char>(size_t(L.R) * L.slot * esize);
-  L.ca = cv.take<char>(size_t(L.plane) * esize);
-  L.cb = cv.take<char>(size_t(L.plane) * esize);
-  const size_t m = size_t(p->npml), nx = size_t(p->nx), ny = size_t(p->ny);
-  const size_t pe[4] = {m * (ny - 2), m * (ny - 2), (nx - 2) * m, (nx - 2) * m};
-  for (int k = 0; k < 4; ++k) L.psi_e[k] = cv.take<char>(std::max<size_t>(pe[k], 1) * esize);
-  const size_t ph[4] = {m * ny, m * ny, nx * m, nx * m};
-  for (int k = 0; k < 8; ++k) L.psi_h[k] = cv.take<char>(std::max<size_t>(ph[k / 2], 1) * esize);
-  L.psi_end = cv.take<char>(0);
-  const int counts[5] = {p->n_sources, p->n_ports, p->n_mx, p->n_my, p->n_probes};
-  for (int k = 0; k < 5; ++k) {
-    L.off[k] = cv.take<int>(L.n_tiles + 1);
-    L.pts[k] = cv.take<Pt>(2 * size_t(std::max(counts[k], 1)));
-  }
-  L.mons = cv.take<Mon>(size_t(std::max(p->n_monitors, 3)));
-  L.step = cv.take<int>(1);
-  L.eacc = cv.take<double>(p->record_energy ? 2 * size_t(std::max(p->n_steps, 1)) : 1);
-  L.total = cv.bytes();
-  return L;
-}
-
 // The gdn_tm_run_f32 time loop with the static scratch, launched eagerly
 // (no CUDA graph is instantiated, since instantiation may allocate).
 static int run_noalloc_f32(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuffers* b,
@@ -965,191 +1312,27 @@ static int run_noalloc_f32(const GdnTmParams* p, const GdnTmPoints* pts, const G
   using T = float;
   int st = validate(p, pts, b);
   if (st) return st;
-  // Largest fold length whose layout fits the static scratch.
-  Layout L = make_layout_fold(p, sizeof(T), 32);
-  if (p->n_freq > 0)
-    for (int t = 32; t >= 2 && L.total > kStaticScratchBytes; --t)
-      L = make_layout_fold(p, sizeof(T), t);
-  if (L.total > kStaticScratchBytes)
+  if ((st = set_kernel_attributes<T>())) return st;
+  // Largest monitor-ring length (a multiple of TB) whose layout fits.
+  Run<T> R;
+  R.L = make_layout(p, pts, sizeof(T));
+  const int tb = R.L.cfg.tb;
+  for (int r = R.L.R; r > tb && R.L.total > kStaticScratchBytes; r -= tb)
+    R.L = make_layout(p, pts, sizeof(T), r - tb);
+  if (R.L.total > kStaticScratchBytes)
     GDN_BAD_ARG("this run needs %zu bytes of scratch; the static scratch of "
                 "gdn_tm_run_noalloc_f32 holds %zu bytes (use gdn_tm_run_f32)",
-                L.total, kStaticScratchBytes);
+                R.L.total, kStaticScratchBytes);
   char* ws = nullptr;
   if ((st = static_scratch(&ws))) return st;
-
-  const int nx = p->nx, ny = p->ny, N = p->n_steps;
-  Dev<T> d{};
-  d.nx = nx;
-  d.ny = ny;
-  d.ld = L.ld;
-  d.npml = p->npml;
-  d.R = L.R;
-  d.n_steps = N;
-  d.n_freq = p->n_freq;
-  d.plane = L.plane;
-  d.slot = L.slot;
-  d.ring = reinterpret_cast<T*>(ws + L.ring);
-  d.ca = reinterpret_cast<const T*>(ws + L.ca);
-  d.cb = reinterpret_cast<const T*>(ws + L.cb);
-  d.eps = static_cast<const T*>(b->eps);
-  d.ikx_e = static_cast<const T*>(b->inv_kx_e);
-  d.iky_e = static_cast<const T*>(b->inv_ky_e);
-  d.ikx_h = static_cast<const T*>(b->inv_kx_h);
-  d.iky_h = static_cast<const T*>(b->inv_ky_h);
-#define GDN_TAB(x) d.x = static_cast<const T*>(b->x)
-  GDN_TAB(b_ezx_lo); GDN_TAB(c_ezx_lo); GDN_TAB(b_ezx_hi); GDN_TAB(c_ezx_hi);
-  GDN_TAB(b_ezy_lo); GDN_TAB(c_ezy_lo); GDN_TAB(b_ezy_hi); GDN_TAB(c_ezy_hi);
-  GDN_TAB(b_hyx_lo); GDN_TAB(c_hyx_lo); GDN_TAB(b_hyx_hi); GDN_TAB(c_hyx_hi);
-  GDN_TAB(b_hxy_lo); GDN_TAB(c_hxy_lo); GDN_TAB(b_hxy_hi); GDN_TAB(c_hxy_hi);
-#undef GDN_TAB
-  d.ezx_lo = reinterpret_cast<T*>(ws + L.psi_e[0]);
-  d.ezx_hi = reinterpret_cast<T*>(ws + L.psi_e[1]);
-  d.ezy_lo = reinterpret_cast<T*>(ws + L.psi_e[2]);
-  d.ezy_hi = reinterpret_cast<T*>(ws + L.psi_e[3]);
-  for (int par = 0; par < 2; ++par) {
-    d.hyx_lo[par] = reinterpret_cast<T*>(ws + L.psi_h[0 + par]);
-    d.hyx_hi[par] = reinterpret_cast<T*>(ws + L.psi_h[2 + par]);
-    d.hxy_lo[par] = reinterpret_cast<T*>(ws + L.psi_h[4 + par]);
-    d.hxy_hi[par] = reinterpret_cast<T*>(ws + L.psi_h[6 + par]);
-  }
-  d.dt_mu = T(b->dt_mu);
-  d.inv_dx = T(b->inv_dx);
-  d.inv_dy = T(b->inv_dy);
-  d.dx = T(p->dx);
-  d.dy = T(p->dy);
-  d.dz = T(p->dz);
-  d.n_src = p->n_sources;
-  d.n_ports = p->n_ports;
-  d.n_mx = p->n_mx;
-  d.n_my = p->n_my;
-  d.n_probes = p->n_probes;
-  d.cb_src = static_cast<const T*>(b->cb_src);
-  d.src_cur = static_cast<const T*>(b->src_cur);
-  d.cb_vs = static_cast<const T*>(b->cb_vs);
-  d.port_vs = static_cast<const T*>(b->port_vs);
-  d.mx_cur = static_cast<const T*>(b->mx_cur);
-  d.my_cur = static_cast<const T*>(b->my_cur);
-  d.cw = p->cw_sources;
-  d.cw_env = b->cw_env;
-  d.src_w = reinterpret_cast<const double2*>(b->src_w);
-  d.mx_w = reinterpret_cast<const double2*>(b->mx_w);
-  d.my_w = reinterpret_cast<const double2*>(b->my_w);
-  d.ph_e = reinterpret_cast<const double2*>(b->ph_e);
-  d.ph_h = reinterpret_cast<const double2*>(b->ph_h);
-  d.out_probe = static_cast<T*>(b->out_probe);
-  d.out_v = static_cast<T*>(b->out_v);
-  d.out_i = static_cast<T*>(b->out_i);
-  int* step_base = reinterpret_cast<int*>(ws + L.step);
-  d.step_base = step_base;
-
-  const int counts[5] = {p->n_sources, p->n_ports, p->n_mx, p->n_my, p->n_probes};
-  const int32_t* is[5] = {pts->src_i, pts->port_i, pts->mx_i, pts->my_i, pts->probe_i};
-  const int32_t* js[5] = {pts->src_j, pts->port_j, pts->mx_j, pts->my_j, pts->probe_j};
-  const int kinds[5] = {0, 0, 1, 2, 0};
-  const int* offs[5];
-  const Pt* pls[5];
-  for (int k = 0; k < 5; ++k) {
-    Bins bn = bin_tiles(counts[k], is[k], js[k], L, kinds[k]);
-    GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.off[k], bn.off.data(), bn.off.size() * sizeof(int),
-                                 cudaMemcpyHostToDevice, stream));
-    if (!bn.pts.empty())
-      GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.pts[k], bn.pts.data(), bn.pts.size() * sizeof(Pt),
-                                   cudaMemcpyHostToDevice, stream));
-    offs[k] = reinterpret_cast<const int*>(ws + L.off[k]);
-    pls[k] = reinterpret_cast<const Pt*>(ws + L.pts[k]);
-  }
-  d.src_off = offs[0]; d.src_pts = pls[0];
-  d.port_off = offs[1]; d.port_pts = pls[1];
-  d.mx_off = offs[2]; d.mx_pts = pls[2];
-  d.my_off = offs[3]; d.my_pts = pls[3];
-  d.probe_off = offs[4]; d.probe_pts = pls[4];
-
-  // The scratch keeps the previous call's contents: clear all state that the
-  // time loop expects to start at zero (ring incl. ghost cells, padded ca/cb
-  // ghosts, psi slabs, step counter, energy sums).
-  GDN_TRY_CUDA(cudaMemsetAsync(ws + L.ring, 0, L.psi_end - L.ring, stream));
-  GDN_TRY_CUDA(cudaMemsetAsync(step_base, 0, sizeof(int), stream));
-  const int eblocks = int(std::min<long long>(div_up((long long)nx * ny, 256), 148 * 8));
-  tm_pad_in<T><<<eblocks, 256, 0, stream>>>(static_cast<const T*>(b->ca),
-                                             reinterpret_cast<T*>(ws + L.ca), nx, ny, L.ld);
-  tm_pad_in<T><<<eblocks, 256, 0, stream>>>(static_cast<const T*>(b->cb),
-                                             reinterpret_cast<T*>(ws + L.cb), nx, ny, L.ld);
-  double* eacc = reinterpret_cast<double*>(ws + L.eacc);
-  if (p->record_energy)
-    GDN_TRY_CUDA(cudaMemsetAsync(eacc, 0, 2 * size_t(std::max(N, 1)) * sizeof(double), stream));
-
-  const bool f64acc = p->dft_f64 != 0;
-  const size_t csz = f64acc ? sizeof(double2) : sizeof(float2);
-  std::vector<Mon> mons;
-  if (p->n_freq > 0) {
-    if (p->n_monitors == 0) {
-      void* const outs[3] = {b->dft_ez, b->dft_hx, b->dft_hy};
-      const int shp[3][2] = {{nx, ny}, {nx, ny - 1}, {nx - 1, ny}};
-      for (int c = 0; c < 3; ++c)
-        mons.push_back(Mon{c, 0, 0, shp[c][1], (long long)shp[c][0] * shp[c][1], outs[c]});
-    } else {
-      for (int k = 0; k < p->n_monitors; ++k) {
-        const GdnDftMonitor& m = pts->monitors[k];
-        const int h = m.hi[0] - m.lo[0], w = m.hi[1] - m.lo[1];
-        mons.push_back(Mon{m.comp, m.lo[0], m.lo[1], w, (long long)h * w, m.out});
-      }
-    }
-  }
-  long long max_cells = 0;
-  for (const Mon& m : mons) {
-    max_cells = std::max(max_cells, m.count);
-    GDN_TRY_CUDA(cudaMemsetAsync(m.out, 0, size_t(m.count) * p->n_freq * csz, stream));
-  }
-  const Mon* d_mons = reinterpret_cast<const Mon*>(ws + L.mons);
-  if (!mons.empty())
-    GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.mons, mons.data(), mons.size() * sizeof(Mon),
-                                 cudaMemcpyHostToDevice, stream));
-
-  // Eager time loop: chunks of L.T steps, each closed by the DFT fold and
-  // the counter advance, exactly as the graph of gdn_tm_run_f32 orders them.
-  const dim3 grd(L.tiles_x, L.tiles_y);
-  uint64_t launched = 2;
-  for (int base = 0; base < N; base += L.T) {
-    const int cnt = std::min(L.T, N - base);
-    for (int s = 0; s < cnt; ++s) {
-      tm_step<T><<<grd, NT, 0, stream>>>(d, s);
-      ++launched;
-      if (p->record_energy) {
-        tm_energy<T><<<eblocks, 256, 0, stream>>>(d, eacc, s);
-        ++launched;
-      }
-    }
-    if (!mons.empty()) {
-      const dim3 dg(unsigned(div_up(max_cells, 256)), unsigned(mons.size()));
-      if (f64acc)
-        tm_dft_fold<T, double><<<dg, 256, size_t(4) * cnt * p->n_freq * sizeof(double), stream>>>(
-            d, d_mons, 0, cnt);
-      else
-        tm_dft_fold<T, float><<<dg, 256, size_t(4) * cnt * p->n_freq * sizeof(float), stream>>>(
-            d, d_mons, 0, cnt);
-      ++launched;
-    }
-    tm_advance<<<1, 1, 0, stream>>>(step_base, cnt);
-    ++launched;
-  }
-
-  const T* last = d.ring + (long long)(N % L.R) * L.slot;
-  tm_copy_out<T><<<eblocks, 256, 0, stream>>>(last, L.plane, nx, ny, L.ld, static_cast<T*>(b->ez),
-                                              static_cast<T*>(b->hx), static_cast<T*>(b->hy));
-  for (const Mon& m : mons) {
-    const long long cnt = m.count * p->n_freq;
-    const int blocks = int(std::min<long long>(div_up(cnt, 256), 148 * 8));
-    if (f64acc)
-      tm_dft_scale<double2><<<blocks, 256, 0, stream>>>(static_cast<double2*>(m.out), cnt, p->dt);
-    else
-      tm_dft_scale<float2><<<blocks, 256, 0, stream>>>(static_cast<float2*>(m.out), cnt, p->dt);
-  }
-  if (p->record_energy && N > 0)
-    tm_energy_finish<T><<<unsigned(div_up(N, 256)), 256, 0, stream>>>(
-        eacc, static_cast<T*>(b->out_energy), N, p->dx * p->dy, p->mu0);
-  count_launches(launched + 1 + mons.size() + (p->record_energy && N > 0 ? 1 : 0));
-  GDN_TRY_CUDA(cudaGetLastError());
-  return GDN_OK;
+  // The scratch keeps the previous call's contents; prepare() clears all
+  // state that the time loop expects to start at zero.
+  if ((st = prepare(p, pts, b, ws, R, stream))) return st;
+  uint64_t launched = 0;
+  for (int base = 0; base < p->n_steps; base += R.L.R)
+    launched += enqueue_chunk(R, p, std::min(R.L.R, p->n_steps - base), stream);
+  count_launches(launched);
+  return finalize(p, b, R, stream);
 }
 
 }  // namespace tm2d

@@ -467,7 +467,8 @@ def simulate_tm(
 
     f64 = fdt == torch.float64
     nbytes = ctypes.c_size_t(0)
-    _native.check(lib.gdn_tm_workspace_size(ctypes.byref(params), int(f64), ctypes.byref(nbytes)))
+    _native.check(lib.gdn_tm_workspace_size(ctypes.byref(params), ctypes.byref(pts), int(f64),
+                                            ctypes.byref(nbytes)))
     ws = torch.empty(max(int(nbytes.value), 1), dtype=torch.uint8, device=dev)
     bufs.workspace, bufs.workspace_bytes = ws.data_ptr(), int(nbytes.value)
 

@@ -150,8 +150,10 @@ typedef struct GdnTmBuffers {
   size_t workspace_bytes;
 } GdnTmBuffers;
 
-/* Scratch bytes needed by gdn_tm_run_* for these parameters. */
-int gdn_tm_workspace_size(const GdnTmParams* p, int f64, size_t* bytes);
+/* Scratch bytes needed by gdn_tm_run_* for these parameters and points (the
+ * monitor list sizes the DFT monitor ring; pts may be NULL without
+ * monitors). */
+int gdn_tm_workspace_size(const GdnTmParams* p, const GdnTmPoints* pts, int f64, size_t* bytes);
 
 /* Run the whole 2D TM time loop (replaces gradenna_tm_run_f32/_f64,
  * rust/src/lib.rs:89-641). Stream-ordered; host index lists are consumed

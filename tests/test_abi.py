@@ -66,7 +66,7 @@ def test_bad_arguments_return_status_not_abort():
     p = _native.TmParams()
     p.nx, p.ny, p.npml = 2, 2, 0
     nbytes = ctypes.c_size_t(0)
-    assert lib.gdn_tm_workspace_size(ctypes.byref(p), 0, ctypes.byref(nbytes)) == 1
+    assert lib.gdn_tm_workspace_size(ctypes.byref(p), None, 0, ctypes.byref(nbytes)) == 1
     assert b"grid" in lib.gdn_last_error()
     # A grid too small for its CPML is rejected before any device work.
     p.nx, p.ny, p.npml, p.n_steps = 20, 20, 10, 5
