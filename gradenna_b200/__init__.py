@@ -9,6 +9,7 @@ array type.
 from gradenna_b200.constants import C0, EPS0, ETA0, MU0
 from gradenna_b200.cpml import CPMLSpec, alpha_max_for_fmin, axis_coefficients
 from gradenna_b200.fdtd2d import DZ, Port, SimResult, simulate_tm
+from gradenna_b200.fdtd3d import DFTMonitor, SimResult3D, port_impedance, simulate_3d, time_series_dft
 from gradenna_b200.grid import Grid2D, Grid3D
 from gradenna_b200.sources import gaussian, gaussian_derivative, modulated_gaussian
 
@@ -16,6 +17,7 @@ __all__ = [
     "C0", "EPS0", "ETA0", "MU0",
     "CPMLSpec", "alpha_max_for_fmin", "axis_coefficients",
     "DZ", "Port", "SimResult", "simulate_tm",
+    "DFTMonitor", "SimResult3D", "simulate_3d", "time_series_dft", "port_impedance",
     "Grid2D", "Grid3D",
     "gaussian", "gaussian_derivative", "modulated_gaussian",
 ]

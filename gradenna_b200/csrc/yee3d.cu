@@ -1,0 +1,824 @@
+// 3D Yee FDTD time loop for B200 (sm_100a).
+//
+// Replaces the reference's fused CPU kernel gradenna_3d_run_f32/_f64
+// (rust/src/lib3d.rs:191-828, lib3d_sweeps.rs) and the scan body of
+// simulate_3d (src/gradenna/fdtd3d.py:559-679) with the same per-step
+// order: H (Hx, Hy, Hz with 6 slab psi) -> Mx/My/Mz -> port Ampere current ->
+// Ex (+Jx), Ey (+Jy), Ez (+Jz) with 6 psi -> semi-implicit RVS overwrite of
+// the port edge -> DFT -> probes / V / energy.
+//
+// B200 design: two kernels per step updating in place (the H kernel reads
+// only E and the E kernel only H, so no CTA ever reads a value another CTA is
+// writing). A CTA covers a 1 x 8 x 32 (i, j, k) box with k contiguous, so
+// every field access is a coalesced row. CPML psi lives in full padded
+// volumes (zero outside the slabs) indexed like the fields; only slab cells
+// touch them. Point work (sources, the port, probes) is binned by CTA box on
+// the host and applied by the owning CTA after its sweep. The running DFT
+// uses the monitor ring of the 2D path: each step the owning CTA writes the
+// monitored cells to ring slot n % R, and one fold kernel per R steps adds
+// sum_t ph[t,k] x_t to the accumulators. One chunk of R steps is captured as
+// a CUDA graph and replayed; kernels read the absolute step from a counter.
+#include <algorithm>
+#include <cmath>
+
+#include "common.cuh"
+
+namespace gdn {
+namespace yee3d {
+
+constexpr int BK = 32, BJ = 8;  // CTA box along k and j (one i-plane)
+constexpr int NT = BK * BJ;
+constexpr int KMAX = 16;
+constexpr int NC = 6;  // components: ex ey ez hx hy hz
+
+struct Pt3 {
+  int m, i, j, k;
+};
+
+struct Mon3 {
+  int comp, lo0, lo1, lo2, s0, s1, s2, pad;
+  long long count, off;
+  void* out;
+};
+
+template <typename T>
+struct Dev3 {
+  int nx, ny, nz, npml, n_steps, n_freq, R, gj, gk;  // gj, gk: CTA grid along j, k
+  int sy, sz;          // padded strides: cell (i,j,k) at ((i+1)*sy + (j+1))*sz + (k+1)
+  long long vol;       // elements per padded volume
+  T* f[NC];            // fields
+  T* psi;              // 12 padded volumes (see psi_* constants)
+  const T *ca, *cb, *eps;  // caller (nx, ny, nz)
+  const T *ik_e[3], *ik_h[3];
+  const T *be_lo[3], *ce_lo[3], *be_hi[3], *ce_hi[3];
+  const T *bh_lo[3], *ch_lo[3], *bh_hi[3], *ch_hi[3];
+  T dt_mu, inv_d[3], dx, dy, dz, a_port, b_port, c_port;
+  int n_src, n_jx, n_jy, n_mx, n_my, n_mz, n_probes, has_port, pi, pj, pk;
+  int port_cta;
+  const int* off[7];  // per point type CSR over CTAs: src jx jy mx my mz probe
+  const Pt3* pts[7];
+  const T *cb_src, *cb_jx, *cb_jy;
+  const T* cur[6];  // src jx jy mx my mz
+  const T* port_vs;
+  int cw;
+  const double* cw_env;
+  const double2* w[6];
+  const double2 *ph_e, *ph_h;
+  T *out_probe, *out_v, *out_i;
+  T* mring;
+  long long mon_cells;
+  int n_mons;
+  const Mon3* mons;
+  const int* step_base;
+};
+
+// psi volume order: field x stretched axis.
+enum { P_EXY, P_EXZ, P_EYX, P_EYZ, P_EZX, P_EZY, P_HXY, P_HXZ, P_HYX, P_HYZ, P_HZX, P_HZY };
+
+template <typename T>
+__device__ __forceinline__ long long at(const Dev3<T>& d, int i, int j, int k) {
+  return ((long long)(i + 1) * d.sy + (j + 1)) * d.sz + (k + 1);
+}
+
+template <typename T>
+__device__ __forceinline__ T wave(const Dev3<T>& d, int type, int n_pts, int m, int n) {
+  if (!d.cw) return d.cur[type][(long long)n * n_pts + m];
+  double s = 0.0;
+  const double2* ph = type <= 2 ? d.ph_e : d.ph_h;
+  for (int k = 0; k < d.n_freq; ++k) {
+    const double2 a = d.w[type][(long long)m * d.n_freq + k];
+    const double2 p = ph[(long long)n * d.n_freq + k];
+    s += a.x * p.x + a.y * p.y;
+  }
+  return T(d.cw_env[n] * s);
+}
+
+// CPML term of one derivative along axis `ax` at sample index `s` of that
+// axis (E-type: s = node - 1 on the PEC interior of n-2 samples; H-type: s
+// on the n-1 half samples): psi <- b psi + c diff, returns diff/kappa + psi
+// inside a slab and diff outside (cpml.py:120-158).
+template <typename T, bool E>
+__device__ __forceinline__ T cpml(const Dev3<T>& d, int ax, int s, int n_samples, T diff,
+                                  T* psi) {
+  const int m = d.npml;
+  if (s < m) {
+    const T p = (E ? d.be_lo[ax][s] : d.bh_lo[ax][s]) * *psi +
+                (E ? d.ce_lo[ax][s] : d.ch_lo[ax][s]) * diff;
+    *psi = p;
+    return diff * (E ? d.ik_e[ax][s] : d.ik_h[ax][s]) + p;
+  }
+  if (s >= n_samples - m) {
+    const int t = s - (n_samples - m);
+    const T p = (E ? d.be_hi[ax][t] : d.bh_hi[ax][t]) * *psi +
+                (E ? d.ce_hi[ax][t] : d.ch_hi[ax][t]) * diff;
+    *psi = p;
+    return diff * (E ? d.ik_e[ax][s] : d.ik_h[ax][s]) + p;
+  }
+  return diff;
+}
+
+// Monitored cells of this CTA's box for components in [c0, c1).
+template <typename T>
+__device__ __forceinline__ void write_monitors(const Dev3<T>& d, int c0, int c1, int n, int i,
+                                               int j, int k) {
+  if (d.n_mons == 0) return;
+  T* slot = d.mring + (long long)(n % d.R) * d.mon_cells;
+  for (int mm = 0; mm < d.n_mons; ++mm) {
+    const Mon3 mo = d.mons[mm];
+    if (mo.comp < c0 || mo.comp >= c1) continue;
+    const int a = i - mo.lo0, b = j - mo.lo1, c = k - mo.lo2;
+    if (a < 0 || a >= mo.s0 || b < 0 || b >= mo.s1 || c < 0 || c >= mo.s2) continue;
+    slot[mo.off + ((long long)a * mo.s1 + b) * mo.s2 + c] = d.f[mo.comp][at(d, i, j, k)];
+  }
+}
+
+// ---------------------------------------------------------------------------
+// H update: E^n -> H^{n+1/2} (fdtd3d.py:564-588) + Mx/My/Mz + H monitors.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(NT) yee_h(Dev3<T> d, int sub) {
+  const int n = *d.step_base + sub;
+  const int k = blockIdx.x * BK + threadIdx.x;
+  const int j = blockIdx.y * BJ + threadIdx.y;
+  const int i = blockIdx.z;
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  const T *ex = d.f[0], *ey = d.f[1], *ez = d.f[2];
+  T *hx = d.f[3], *hy = d.f[4], *hz = d.f[5];
+  if (j < ny && k < nz) {
+    const long long c = at(d, i, j, k);
+    const long long dj = d.sz, di = (long long)d.sy * d.sz;
+    // Hx (nx, ny-1, nz-1): +dt/mu (t_hxz - t_hxy)
+    if (j < ny - 1 && k < nz - 1) {
+      const T dey_dz = (ey[c + 1] - ey[c]) * d.inv_d[2];
+      const T dez_dy = (ez[c + dj] - ez[c]) * d.inv_d[1];
+      const T tz = cpml<T, false>(d, 2, k, nz - 1, dey_dz, d.psi + P_HXZ * d.vol + c);
+      const T ty = cpml<T, false>(d, 1, j, ny - 1, dez_dy, d.psi + P_HXY * d.vol + c);
+      hx[c] = hx[c] + d.dt_mu * (tz - ty);
+    }
+    // Hy (nx-1, ny, nz-1): +dt/mu (t_hyx - t_hyz)
+    if (i < nx - 1 && k < nz - 1) {
+      const T dez_dx = (ez[c + di] - ez[c]) * d.inv_d[0];
+      const T dex_dz = (ex[c + 1] - ex[c]) * d.inv_d[2];
+      const T tx = cpml<T, false>(d, 0, i, nx - 1, dez_dx, d.psi + P_HYX * d.vol + c);
+      const T tz = cpml<T, false>(d, 2, k, nz - 1, dex_dz, d.psi + P_HYZ * d.vol + c);
+      hy[c] = hy[c] + d.dt_mu * (tx - tz);
+    }
+    // Hz (nx-1, ny-1, nz): +dt/mu (t_hzy - t_hzx)
+    if (i < nx - 1 && j < ny - 1) {
+      const T dex_dy = (ex[c + dj] - ex[c]) * d.inv_d[1];
+      const T dey_dx = (ey[c + di] - ey[c]) * d.inv_d[0];
+      const T ty = cpml<T, false>(d, 1, j, ny - 1, dex_dy, d.psi + P_HZY * d.vol + c);
+      const T tx = cpml<T, false>(d, 0, i, nx - 1, dey_dx, d.psi + P_HZX * d.vol + c);
+      hz[c] = hz[c] + d.dt_mu * (ty - tx);
+    }
+  }
+  const int cta = (i * d.gj + blockIdx.y) * d.gk + blockIdx.x;
+  const int tid = threadIdx.y * BK + threadIdx.x;
+  bool any = false;
+  for (int t = 3; t < 6; ++t) any |= d.off[t][cta] < d.off[t][cta + 1];
+  if (any) {
+    __syncthreads();
+    T* hs[3] = {hx, hy, hz};
+    for (int t = 3; t < 6; ++t) {
+      const int np_ = t == 3 ? d.n_mx : (t == 4 ? d.n_my : d.n_mz);
+      for (int q = d.off[t][cta] + tid; q < d.off[t][cta + 1]; q += NT) {
+        const Pt3 p = d.pts[t][q];
+        atomicAdd(hs[t - 3] + at(d, p.i, p.j, p.k), -(d.dt_mu * wave(d, t, np_, p.m, n)));
+      }
+    }
+  }
+  if (d.n_mons > 0) {
+    __syncthreads();
+    if (j < ny && k < nz) write_monitors(d, 3, 6, n, i, j, k);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// E update: H^{n+1/2} -> E^{n+1} (fdtd3d.py:596-633) + sources, port,
+// probes, V/I and E monitors.
+// ---------------------------------------------------------------------------
+template <typename T>
+__global__ void __launch_bounds__(NT) yee_e(Dev3<T> d, int sub) {
+  __shared__ T s_port[2];  // Ez^n and curl_z at the port edge
+  const int n = *d.step_base + sub;
+  const int k = blockIdx.x * BK + threadIdx.x;
+  const int j = blockIdx.y * BJ + threadIdx.y;
+  const int i = blockIdx.z;
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  T *ex = d.f[0], *ey = d.f[1], *ez = d.f[2];
+  const T *hx = d.f[3], *hy = d.f[4], *hz = d.f[5];
+  const int cta = (i * d.gj + blockIdx.y) * d.gk + blockIdx.x;
+  const bool port_here = d.has_port && cta == d.port_cta;
+  if (j < ny && k < nz) {
+    const long long c = at(d, i, j, k);
+    const long long dj = d.sz, di = (long long)d.sy * d.sz;
+    const long long g = ((long long)i * ny + j) * nz + k;  // node coefficients
+    // Ex (nx-1, ny, nz) interior j, k: t_exy - t_exz
+    if (i < nx - 1 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2) {
+      const T dhz_dy = (hz[c] - hz[c - dj]) * d.inv_d[1];
+      const T dhy_dz = (hy[c] - hy[c - 1]) * d.inv_d[2];
+      const T ty = cpml<T, true>(d, 1, j - 1, ny - 2, dhz_dy, d.psi + P_EXY * d.vol + c);
+      const T tz = cpml<T, true>(d, 2, k - 1, nz - 2, dhy_dz, d.psi + P_EXZ * d.vol + c);
+      ex[c] = d.ca[g] * ex[c] + d.cb[g] * (ty - tz);
+    }
+    // Ey (nx, ny-1, nz) interior i, k: t_eyz - t_eyx
+    if (i >= 1 && i <= nx - 2 && j < ny - 1 && k >= 1 && k <= nz - 2) {
+      const T dhx_dz = (hx[c] - hx[c - 1]) * d.inv_d[2];
+      const T dhz_dx = (hz[c] - hz[c - di]) * d.inv_d[0];
+      const T tz = cpml<T, true>(d, 2, k - 1, nz - 2, dhx_dz, d.psi + P_EYZ * d.vol + c);
+      const T tx = cpml<T, true>(d, 0, i - 1, nx - 2, dhz_dx, d.psi + P_EYX * d.vol + c);
+      ey[c] = d.ca[g] * ey[c] + d.cb[g] * (tz - tx);
+    }
+    // Ez (nx, ny, nz-1) interior i, j: t_ezx - t_ezy
+    if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k < nz - 1) {
+      const T dhy_dx = (hy[c] - hy[c - di]) * d.inv_d[0];
+      const T dhx_dy = (hx[c] - hx[c - dj]) * d.inv_d[1];
+      const T tx = cpml<T, true>(d, 0, i - 1, nx - 2, dhy_dx, d.psi + P_EZX * d.vol + c);
+      const T ty = cpml<T, true>(d, 1, j - 1, ny - 2, dhx_dy, d.psi + P_EZY * d.vol + c);
+      const T curl = tx - ty;
+      if (port_here && i == d.pi && j == d.pj && k == d.pk) {
+        s_port[0] = ez[c];
+        s_port[1] = curl;
+      }
+      ez[c] = d.ca[g] * ez[c] + d.cb[g] * curl;
+    }
+  }
+  const int tid = threadIdx.y * BK + threadIdx.x;
+  bool any = port_here;
+  for (int t = 0; t < 3; ++t) any |= d.off[t][cta] < d.off[t][cta + 1];
+  any |= d.off[6][cta] < d.off[6][cta + 1];
+  if (any) {
+    __syncthreads();
+    T* es[3] = {ez, ex, ey};  // point types 0 src (Jz), 1 jx, 2 jy
+    const T* cbs[3] = {d.cb_src, d.cb_jx, d.cb_jy};
+    const int nps[3] = {d.n_src, d.n_jx, d.n_jy};
+    for (int t = 0; t < 3; ++t)
+      for (int q = d.off[t][cta] + tid; q < d.off[t][cta + 1]; q += NT) {
+        const Pt3 p = d.pts[t][q];
+        atomicAdd(es[t] + at(d, p.i, p.j, p.k), -(cbs[t][p.m] * wave(d, t, nps[t], p.m, n)));
+      }
+    __syncthreads();
+    if (port_here && tid == 0) {
+      const long long c = at(d, d.pi, d.pj, d.pk);
+      const T ez_new = d.a_port * s_port[0] + d.b_port * s_port[1] + d.c_port * d.port_vs[n];
+      ez[c] = ez_new;
+      d.out_v[n] = T(-0.5) * d.dz * (s_port[0] + ez_new);
+      const long long dj = d.sz, di = (long long)d.sy * d.sz;
+      d.out_i[n] = (hy[c] - hy[c - di]) * d.dy + (hx[c - dj] - hx[c]) * d.dx;
+    }
+    __syncthreads();
+    for (int q = d.off[6][cta] + tid; q < d.off[6][cta + 1]; q += NT) {
+      const Pt3 p = d.pts[6][q];
+      d.out_probe[(long long)n * d.n_probes + p.m] = ez[at(d, p.i, p.j, p.k)];
+    }
+  }
+  if (d.n_mons > 0) {
+    __syncthreads();
+    if (j < ny && k < nz) write_monitors(d, 0, 3, n, i, j, k);
+  }
+}
+
+// DFT fold over `cnt` ring slots (fdtd3d.py:635-662).
+template <typename T, typename A, int KM>
+__global__ void __launch_bounds__(256) yee_fold(Dev3<T> d, int cnt) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  A* sph = reinterpret_cast<A*>(smem_raw);
+  using C = typename Cplx<A>::type;
+  const int n0 = *d.step_base;
+  const int K = d.n_freq;
+  for (int idx = threadIdx.x; idx < cnt * K; idx += blockDim.x) {
+    const int t = idx / K, kk = idx - t * K;
+    const double2 pe = d.ph_e[(long long)(n0 + t) * K + kk];
+    const double2 ph = d.ph_h[(long long)(n0 + t) * K + kk];
+    sph[2 * idx] = A(pe.x);
+    sph[2 * idx + 1] = A(pe.y);
+    sph[2 * (cnt * K + idx)] = A(ph.x);
+    sph[2 * (cnt * K + idx) + 1] = A(ph.y);
+  }
+  __syncthreads();
+  const Mon3 mon = d.mons[blockIdx.y];
+  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= mon.count) return;
+  const A* ph = sph + (mon.comp < 3 ? 0 : 2 * cnt * K);
+  A are[KM], aim[KM];
+#pragma unroll
+  for (int kk = 0; kk < KM; ++kk) are[kk] = aim[kk] = A(0);
+  const T* base = d.mring + mon.off + r;
+#pragma unroll 4
+  for (int t = 0; t < cnt; ++t) {
+    const A x = A(base[(long long)((n0 + t) % d.R) * d.mon_cells]);
+#pragma unroll
+    for (int kk = 0; kk < KM; ++kk)
+      if (kk < K) {
+        are[kk] += ph[2 * (t * K + kk)] * x;
+        aim[kk] += ph[2 * (t * K + kk) + 1] * x;
+      }
+  }
+  C* acc = static_cast<C*>(mon.out) + r;
+#pragma unroll
+  for (int kk = 0; kk < KM; ++kk)
+    if (kk < K) {
+      C v = acc[(long long)kk * mon.count];
+      v.x += are[kk];
+      v.y += aim[kk];
+      acc[(long long)kk * mon.count] = v;
+    }
+}
+
+// Total field energy (fdtd3d.py:171-183) of the state after step n.
+template <typename T>
+__global__ void yee_energy(Dev3<T> d, double* eacc, int sub) {
+  const int n = *d.step_base + sub;
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  double ue = 0.0, uh = 0.0;
+  const long long total = (long long)nx * ny * nz;
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
+       g += (long long)gridDim.x * blockDim.x) {
+    const int i = int(g / ((long long)ny * nz));
+    const int rem = int(g - (long long)i * ny * nz);
+    const int j = rem / nz, k = rem - j * nz;
+    const long long c = at(d, i, j, k);
+    const double ep = double(d.eps[g]);
+    const double a = double(d.f[0][c]), b = double(d.f[1][c]), e = double(d.f[2][c]);
+    ue += ep * (a * a + b * b + e * e);  // components are zero outside their grids
+    const double x = double(d.f[3][c]), y = double(d.f[4][c]), z = double(d.f[5][c]);
+    uh += x * x + y * y + z * z;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    ue += __shfl_down_sync(0xffffffffu, ue, o);
+    uh += __shfl_down_sync(0xffffffffu, uh, o);
+  }
+  __shared__ double sue[32], suh[32];
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  if (lane == 0) {
+    sue[wid] = ue;
+    suh[wid] = uh;
+  }
+  __syncthreads();
+  if (wid == 0) {
+    const int nw = blockDim.x >> 5;
+    ue = lane < nw ? sue[lane] : 0.0;
+    uh = lane < nw ? suh[lane] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) {
+      ue += __shfl_down_sync(0xffffffffu, ue, o);
+      uh += __shfl_down_sync(0xffffffffu, uh, o);
+    }
+    if (lane == 0) {
+      atomicAdd(eacc + 2 * n, ue);
+      atomicAdd(eacc + 2 * n + 1, uh);
+    }
+  }
+}
+
+template <typename T>
+__global__ void yee_energy_finish(const double* eacc, T* out, int n_steps, double cell, double mu0) {
+  const int n = blockIdx.x * blockDim.x + threadIdx.x;
+  if (n < n_steps) out[n] = T(0.5 * cell * eacc[2 * n] + 0.5 * mu0 * cell * eacc[2 * n + 1]);
+}
+
+__global__ void yee_advance(int* step_base, int cnt) { *step_base += cnt; }
+
+// Final fields into the caller's unpadded component arrays.
+template <typename T>
+__global__ void yee_copy_out(Dev3<T> d, T* e0, T* e1, T* e2, T* h0, T* h1, T* h2) {
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  const long long total = (long long)nx * ny * nz;
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < total;
+       g += (long long)gridDim.x * blockDim.x) {
+    const int i = int(g / ((long long)ny * nz));
+    const int rem = int(g - (long long)i * ny * nz);
+    const int j = rem / nz, k = rem - j * nz;
+    const long long c = at(d, i, j, k);
+    if (i < nx - 1) e0[((long long)i * ny + j) * nz + k] = d.f[0][c];
+    if (j < ny - 1) e1[((long long)i * (ny - 1) + j) * nz + k] = d.f[1][c];
+    if (k < nz - 1) e2[((long long)i * ny + j) * (nz - 1) + k] = d.f[2][c];
+    if (j < ny - 1 && k < nz - 1) h0[((long long)i * (ny - 1) + j) * (nz - 1) + k] = d.f[3][c];
+    if (i < nx - 1 && k < nz - 1) h1[((long long)i * ny + j) * (nz - 1) + k] = d.f[4][c];
+    if (i < nx - 1 && j < ny - 1) h2[((long long)i * (ny - 1) + j) * nz + k] = d.f[5][c];
+  }
+}
+
+template <typename C>
+__global__ void yee_dft_scale(C* a, long long count, double s) {
+  for (long long g = (long long)blockIdx.x * blockDim.x + threadIdx.x; g < count;
+       g += (long long)gridDim.x * blockDim.x) {
+    C v = a[g];
+    v.x *= s;
+    v.y *= s;
+    a[g] = v;
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Host side
+// ---------------------------------------------------------------------------
+
+static void comp_shape(int c, int nx, int ny, int nz, int s[3]) {
+  const int sh[6][3] = {{nx - 1, ny, nz},     {nx, ny - 1, nz},     {nx, ny, nz - 1},
+                        {nx, ny - 1, nz - 1}, {nx - 1, ny, nz - 1}, {nx - 1, ny - 1, nz}};
+  for (int a = 0; a < 3; ++a) s[a] = sh[c][a];
+}
+
+struct Layout3 {
+  int sy = 0, sz = 0, gj = 0, gk = 0, n_cta = 0, R = 32;
+  long long vol = 0, mon_cells = 0;
+  size_t fields, psi, zero_end, off[7], pts[7], mons, mring, step, eacc, total;
+};
+
+static long long mon_cells3(const GdnYeeParams* p, const GdnYeePoints* pts) {
+  if (p->n_freq <= 0) return 0;
+  long long c = 0;
+  if (p->n_monitors == 0) {
+    for (int k = 0; k < 6; ++k) {
+      int s[3];
+      comp_shape(k, p->nx, p->ny, p->nz, s);
+      c += (long long)s[0] * s[1] * s[2];
+    }
+    return c;
+  }
+  for (int k = 0; k < p->n_monitors; ++k) {
+    const GdnDftMonitor& m = pts->monitors[k];
+    c += (long long)(m.hi[0] - m.lo[0]) * (m.hi[1] - m.lo[1]) * (m.hi[2] - m.lo[2]);
+  }
+  return c;
+}
+
+static const int32_t* pts_of(const GdnYeePoints* pts, int t) {
+  const int32_t* a[7] = {pts->src, pts->jx, pts->jy, pts->mx, pts->my, pts->mz, pts->probe};
+  return a[t];
+}
+static int count_of(const GdnYeeParams* p, int t) {
+  const int a[7] = {p->n_src, p->n_jx, p->n_jy, p->n_mx, p->n_my, p->n_mz, p->n_probes};
+  return a[t];
+}
+
+static Layout3 make_layout3(const GdnYeeParams* p, const GdnYeePoints* pts, size_t esize) {
+  Layout3 L;
+  L.sz = int(div_up(p->nz + 2, 4) * 4);
+  L.sy = p->ny + 2;
+  L.vol = (long long)(p->nx + 2) * L.sy * L.sz;
+  L.gk = int(div_up(p->nz, BK));
+  L.gj = int(div_up(p->ny, BJ));
+  L.n_cta = p->nx * L.gj * L.gk;
+  L.mon_cells = pts ? mon_cells3(p, pts) : 0;
+  const size_t budget = size_t(2) << 30;
+  long long r = L.mon_cells > 0 ? (long long)(budget / (size_t(L.mon_cells) * esize)) : 32;
+  L.R = int(std::max<long long>(1, std::min<long long>(32, r)));
+  Carve cv;
+  L.fields = cv.take<char>(size_t(NC) * L.vol * esize);
+  L.psi = cv.take<char>(size_t(12) * L.vol * esize);
+  L.step = cv.take<int>(1);
+  L.zero_end = cv.take<char>(0);
+  for (int t = 0; t < 7; ++t) {
+    L.off[t] = cv.take<int>(L.n_cta + 1);
+    L.pts[t] = cv.take<Pt3>(std::max(count_of(p, t), 1));
+  }
+  L.mons = cv.take<Mon3>(std::max(p->n_monitors, 6));
+  L.mring = cv.take<char>(std::max<size_t>(size_t(L.mon_cells) * L.R, 1) * esize);
+  L.eacc = cv.take<double>(p->record_energy ? 2 * size_t(std::max(p->n_steps, 1)) : 1);
+  L.total = cv.bytes();
+  return L;
+}
+
+static int validate3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuffers* b) {
+  if (!p || !pts || !b) GDN_BAD_ARG("null params/points/buffers");
+  const int nx = p->nx, ny = p->ny, nz = p->nz;
+  if (std::min({nx, ny, nz}) < 3) GDN_BAD_ARG("grid must be at least 3x3x3");
+  if (p->npml < 0 || std::min({nx, ny, nz}) <= 2 * p->npml + 2)
+    GDN_BAD_ARG("grid %dx%dx%d is too small for CPML thickness %d", nx, ny, nz, p->npml);
+  if (p->n_steps < 0 || p->n_freq < 0 || p->n_freq > KMAX || p->n_monitors < 0)
+    GDN_BAD_ARG("invalid n_steps / n_freq / n_monitors");
+  if ((long long)(nx + 2) * (ny + 2) * (nz + 6) > (1LL << 31))
+    GDN_BAD_ARG("grid too large for 32-bit cell ids");
+  // Source grids: Jz/probe on Ez edges with margin 1 in i, j (fdtd3d.py:246-255);
+  // the other channels anywhere on their own component grid (fdtd3d.py:385-407).
+  const int comp_of[7] = {2, 0, 1, 3, 4, 5, 2};
+  for (int t = 0; t < 7; ++t) {
+    const int n = count_of(p, t);
+    const int32_t* a = pts_of(pts, t);
+    if (n > 0 && !a) GDN_BAD_ARG("point list %d is null", t);
+    int s[3];
+    comp_shape(comp_of[t], nx, ny, nz, s);
+    const int margin = t == 0 ? 1 : 0;
+    for (int m = 0; m < n; ++m) {
+      const int i = a[3 * m], j = a[3 * m + 1], k = a[3 * m + 2];
+      if (i < margin || j < margin || k < 0 || i > s[0] - 1 - margin || j > s[1] - 1 - margin ||
+          k > s[2] - 1)
+        GDN_BAD_ARG("point (%d, %d, %d) of list %d outside its grid", i, j, k, t);
+    }
+  }
+  if (p->has_port) {
+    const int i = pts->port[0], j = pts->port[1], k = pts->port[2];
+    if (i < 1 || j < 1 || k < 0 || i > nx - 2 || j > ny - 2 || k > nz - 2)
+      GDN_BAD_ARG("port (%d, %d, %d) outside the valid Ez range (margin 1)", i, j, k);
+    if (p->n_steps > 0 && !b->port_vs) GDN_BAD_ARG("port_vs is null");
+    if (p->n_steps > 0 && (!b->out_v || !b->out_i)) GDN_BAD_ARG("port outputs are null");
+  }
+  if (!b->ca || !b->cb) GDN_BAD_ARG("ca/cb are null");
+  for (int a = 0; a < 3; ++a) {
+    if (!b->ik_e[a] || !b->ik_h[a]) GDN_BAD_ARG("1/kappa tables are null");
+    if (p->npml > 0 && (!b->b_e_lo[a] || !b->c_e_lo[a] || !b->b_e_hi[a] || !b->c_e_hi[a] ||
+                        !b->b_h_lo[a] || !b->c_h_lo[a] || !b->b_h_hi[a] || !b->c_h_hi[a]))
+      GDN_BAD_ARG("a CPML slab table is null");
+  }
+  if (!b->ex || !b->ey || !b->ez || !b->hx || !b->hy || !b->hz) GDN_BAD_ARG("field outputs are null");
+  if (p->n_probes > 0 && p->n_steps > 0 && !b->out_probe) GDN_BAD_ARG("out_probe is null");
+  if (p->record_energy && p->n_steps > 0 && (!b->out_energy || !b->eps))
+    GDN_BAD_ARG("energy buffers are null");
+  if (p->n_freq > 0 && p->n_steps > 0 && (!b->ph_e || !b->ph_h)) GDN_BAD_ARG("phase tables are null");
+  if (p->n_freq > 0 && p->n_monitors == 0)
+    for (int c = 0; c < 6; ++c)
+      if (!b->dft[c]) GDN_BAD_ARG("full-grid dft output %d is null", c);
+  if (p->n_freq > 0 && p->n_monitors > 0) {
+    if (!pts->monitors) GDN_BAD_ARG("monitor list is null");
+    for (int k = 0; k < p->n_monitors; ++k) {
+      const GdnDftMonitor& m = pts->monitors[k];
+      if (m.comp < 0 || m.comp > 5) GDN_BAD_ARG("monitor %d: component %d", k, m.comp);
+      int s[3];
+      comp_shape(m.comp, nx, ny, nz, s);
+      for (int a = 0; a < 3; ++a)
+        if (m.lo[a] < 0 || m.hi[a] > s[a] || m.hi[a] <= m.lo[a])
+          GDN_BAD_ARG("monitor %d: box empty or outside component %d", k, m.comp);
+      if (!m.out) GDN_BAD_ARG("monitor %d: output is null", k);
+    }
+  }
+  if (p->cw_sources && (p->n_freq <= 0 || !b->cw_env)) GDN_BAD_ARG("cw_sources needs n_freq and cw_env");
+  if (p->n_steps > 0) {
+    const void* cur[6] = {b->src_cur, b->jx_cur, b->jy_cur, b->mx_cur, b->my_cur, b->mz_cur};
+    const double* w[6] = {b->src_w, b->jx_w, b->jy_w, b->mx_w, b->my_w, b->mz_w};
+    for (int t = 0; t < 6; ++t)
+      if (count_of(p, t) > 0 && (p->cw_sources ? !w[t] : !cur[t]))
+        GDN_BAD_ARG("waveform of point list %d is null", t);
+  }
+  if ((p->n_src && !b->cb_src) || (p->n_jx && !b->cb_jx) || (p->n_jy && !b->cb_jy))
+    GDN_BAD_ARG("source coefficients are null");
+  if (p->dt <= 0 || p->dx <= 0 || p->dy <= 0 || p->dz <= 0) GDN_BAD_ARG("dt, dx, dy, dz must be positive");
+  return GDN_OK;
+}
+
+template <typename T, typename A>
+static void launch_fold3(const Dev3<T>& d, const std::vector<Mon3>& mons, long long max_cells,
+                         int cnt, int K, cudaStream_t s) {
+  const dim3 dg(unsigned(div_up(max_cells, 256)), unsigned(mons.size()));
+  const size_t sm = size_t(4) * cnt * K * sizeof(A);
+  if (K <= 4)
+    yee_fold<T, A, 4><<<dg, 256, sm, s>>>(d, cnt);
+  else if (K <= 8)
+    yee_fold<T, A, 8><<<dg, 256, sm, s>>>(d, cnt);
+  else
+    yee_fold<T, A, KMAX><<<dg, 256, sm, s>>>(d, cnt);
+}
+
+template <typename T>
+static int run3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuffers* b,
+                cudaStream_t stream) {
+  int st = validate3(p, pts, b);
+  if (st) return st;
+  const Layout3 L = make_layout3(p, pts, sizeof(T));
+  char* ws = static_cast<char*>(b->workspace);
+  bool own = false;
+  if (!ws) {
+    GDN_TRY_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&ws), L.total, stream));
+    own = true;
+  } else if (b->workspace_bytes < L.total) {
+    GDN_BAD_ARG("workspace too small: %zu < %zu bytes", b->workspace_bytes, L.total);
+  }
+  struct Guard {
+    char* p;
+    bool own;
+    cudaStream_t s;
+    ~Guard() {
+      if (own && p) cudaFreeAsync(p, s);
+    }
+  } guard{ws, own, stream};
+
+  const int nx = p->nx, ny = p->ny, nz = p->nz, N = p->n_steps;
+  Dev3<T> d{};
+  d.nx = nx; d.ny = ny; d.nz = nz; d.npml = p->npml; d.n_steps = N; d.n_freq = p->n_freq;
+  d.R = L.R; d.gj = L.gj; d.gk = L.gk; d.sy = L.sy; d.sz = L.sz; d.vol = L.vol;
+  for (int c = 0; c < NC; ++c) d.f[c] = reinterpret_cast<T*>(ws + L.fields) + c * L.vol;
+  d.psi = reinterpret_cast<T*>(ws + L.psi);
+  d.ca = static_cast<const T*>(b->ca);
+  d.cb = static_cast<const T*>(b->cb);
+  d.eps = static_cast<const T*>(b->eps);
+  for (int a = 0; a < 3; ++a) {
+    d.ik_e[a] = static_cast<const T*>(b->ik_e[a]);
+    d.ik_h[a] = static_cast<const T*>(b->ik_h[a]);
+    d.be_lo[a] = static_cast<const T*>(b->b_e_lo[a]);
+    d.ce_lo[a] = static_cast<const T*>(b->c_e_lo[a]);
+    d.be_hi[a] = static_cast<const T*>(b->b_e_hi[a]);
+    d.ce_hi[a] = static_cast<const T*>(b->c_e_hi[a]);
+    d.bh_lo[a] = static_cast<const T*>(b->b_h_lo[a]);
+    d.ch_lo[a] = static_cast<const T*>(b->c_h_lo[a]);
+    d.bh_hi[a] = static_cast<const T*>(b->b_h_hi[a]);
+    d.ch_hi[a] = static_cast<const T*>(b->c_h_hi[a]);
+  }
+  d.dt_mu = T(b->dt_mu);
+  d.inv_d[0] = T(b->inv_dx);
+  d.inv_d[1] = T(b->inv_dy);
+  d.inv_d[2] = T(b->inv_dz);
+  d.dx = T(p->dx); d.dy = T(p->dy); d.dz = T(p->dz);
+  d.a_port = T(b->a_port); d.b_port = T(b->b_port); d.c_port = T(b->c_port);
+  d.n_src = p->n_src; d.n_jx = p->n_jx; d.n_jy = p->n_jy;
+  d.n_mx = p->n_mx; d.n_my = p->n_my; d.n_mz = p->n_mz; d.n_probes = p->n_probes;
+  d.has_port = p->has_port;
+  d.pi = pts->port[0]; d.pj = pts->port[1]; d.pk = pts->port[2];
+  d.port_cta = p->has_port ? (d.pi * L.gj + d.pj / BJ) * L.gk + d.pk / BK : -1;
+  d.cb_src = static_cast<const T*>(b->cb_src);
+  d.cb_jx = static_cast<const T*>(b->cb_jx);
+  d.cb_jy = static_cast<const T*>(b->cb_jy);
+  const void* curs[6] = {b->src_cur, b->jx_cur, b->jy_cur, b->mx_cur, b->my_cur, b->mz_cur};
+  const double* ws6[6] = {b->src_w, b->jx_w, b->jy_w, b->mx_w, b->my_w, b->mz_w};
+  for (int t = 0; t < 6; ++t) {
+    d.cur[t] = static_cast<const T*>(curs[t]);
+    d.w[t] = reinterpret_cast<const double2*>(ws6[t]);
+  }
+  d.port_vs = static_cast<const T*>(b->port_vs);
+  d.cw = p->cw_sources;
+  d.cw_env = b->cw_env;
+  d.ph_e = reinterpret_cast<const double2*>(b->ph_e);
+  d.ph_h = reinterpret_cast<const double2*>(b->ph_h);
+  d.out_probe = static_cast<T*>(b->out_probe);
+  d.out_v = static_cast<T*>(b->out_v);
+  d.out_i = static_cast<T*>(b->out_i);
+  d.mring = reinterpret_cast<T*>(ws + L.mring);
+  d.mon_cells = L.mon_cells;
+  int* step_base = reinterpret_cast<int*>(ws + L.step);
+  d.step_base = step_base;
+
+  // Point bins by CTA box (i, j/BJ, k/BK).
+  for (int t = 0; t < 7; ++t) {
+    const int n = count_of(p, t);
+    const int32_t* a = pts_of(pts, t);
+    std::vector<int> off(L.n_cta + 1, 0), cta(n);
+    for (int m = 0; m < n; ++m) {
+      cta[m] = (a[3 * m] * L.gj + a[3 * m + 1] / BJ) * L.gk + a[3 * m + 2] / BK;
+      off[cta[m] + 1]++;
+    }
+    for (int c = 0; c < L.n_cta; ++c) off[c + 1] += off[c];
+    std::vector<Pt3> rec(std::max(n, 1));
+    std::vector<int> cur(off.begin(), off.end() - 1);
+    for (int m = 0; m < n; ++m) rec[cur[cta[m]]++] = Pt3{m, a[3 * m], a[3 * m + 1], a[3 * m + 2]};
+    GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.off[t], off.data(), off.size() * sizeof(int),
+                                 cudaMemcpyHostToDevice, stream));
+    if (n > 0)
+      GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.pts[t], rec.data(), size_t(n) * sizeof(Pt3),
+                                   cudaMemcpyHostToDevice, stream));
+    d.off[t] = reinterpret_cast<const int*>(ws + L.off[t]);
+    d.pts[t] = reinterpret_cast<const Pt3*>(ws + L.pts[t]);
+  }
+
+  // Monitors.
+  const bool f64acc = p->dft_f64 != 0;
+  const size_t csz = f64acc ? sizeof(double2) : sizeof(float2);
+  std::vector<Mon3> mons;
+  if (p->n_freq > 0) {
+    long long off = 0;
+    const int nm = p->n_monitors == 0 ? 6 : p->n_monitors;
+    for (int k = 0; k < nm; ++k) {
+      Mon3 m{};
+      if (p->n_monitors == 0) {
+        int s[3];
+        comp_shape(k, nx, ny, nz, s);
+        m.comp = k;
+        m.s0 = s[0]; m.s1 = s[1]; m.s2 = s[2];
+        m.out = b->dft[k];
+      } else {
+        const GdnDftMonitor& g = pts->monitors[k];
+        m.comp = g.comp;
+        m.lo0 = g.lo[0]; m.lo1 = g.lo[1]; m.lo2 = g.lo[2];
+        m.s0 = g.hi[0] - g.lo[0]; m.s1 = g.hi[1] - g.lo[1]; m.s2 = g.hi[2] - g.lo[2];
+        m.out = g.out;
+      }
+      m.count = (long long)m.s0 * m.s1 * m.s2;
+      m.off = off;
+      off += m.count;
+      mons.push_back(m);
+    }
+  }
+  d.n_mons = int(mons.size());
+  d.mons = reinterpret_cast<const Mon3*>(ws + L.mons);
+  long long max_cells = 0;
+  for (const Mon3& m : mons) {
+    max_cells = std::max(max_cells, m.count);
+    GDN_TRY_CUDA(cudaMemsetAsync(m.out, 0, size_t(m.count) * p->n_freq * csz, stream));
+  }
+  if (!mons.empty())
+    GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.mons, mons.data(), mons.size() * sizeof(Mon3),
+                                 cudaMemcpyHostToDevice, stream));
+  GDN_TRY_CUDA(cudaMemsetAsync(ws + L.fields, 0, L.zero_end - L.fields, stream));
+  double* eacc = reinterpret_cast<double*>(ws + L.eacc);
+  if (p->record_energy)
+    GDN_TRY_CUDA(cudaMemsetAsync(eacc, 0, 2 * size_t(std::max(N, 1)) * sizeof(double), stream));
+
+  const dim3 blk(BK, BJ);
+  const dim3 grd(L.gk, L.gj, nx);
+  const int eblocks = int(std::min<long long>(div_up((long long)nx * ny * nz, 256), 148 * 8));
+  auto enqueue = [&](int cnt, cudaStream_t s) -> uint64_t {
+    uint64_t k = 0;
+    for (int t = 0; t < cnt; ++t) {
+      yee_h<T><<<grd, blk, 0, s>>>(d, t);
+      yee_e<T><<<grd, blk, 0, s>>>(d, t);
+      k += 2;
+      if (p->record_energy) {
+        yee_energy<T><<<eblocks, 256, 0, s>>>(d, eacc, t);
+        ++k;
+      }
+    }
+    if (!mons.empty()) {
+      if (f64acc)
+        launch_fold3<T, double>(d, mons, max_cells, cnt, p->n_freq, s);
+      else
+        launch_fold3<T, float>(d, mons, max_cells, cnt, p->n_freq, s);
+      ++k;
+    }
+    yee_advance<<<1, 1, 0, s>>>(step_base, cnt);
+    return k + 1;
+  };
+  auto capture = [&](int cnt, cudaGraphExec_t* exec, uint64_t* nodes) -> int {
+    cudaStream_t cs = capture_stream();
+    if (!cs) GDN_BAD_ARG("no capture stream for this device");
+    GDN_TRY_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
+    *nodes = enqueue(cnt, cs);
+    cudaGraph_t g = nullptr;
+    const cudaError_t e1 = cudaStreamEndCapture(cs, &g);
+    if (e1 != cudaSuccess) {
+      set_error("graph capture failed: %s", cudaGetErrorString(e1));
+      return GDN_ERR_CUDA;
+    }
+    const cudaError_t e2 = cudaGraphInstantiate(exec, g, 0);
+    cudaGraphDestroy(g);
+    if (e2 != cudaSuccess) {
+      set_error("graph instantiate failed: %s", cudaGetErrorString(e2));
+      return GDN_ERR_CUDA;
+    }
+    return GDN_OK;
+  };
+  const int Tc = L.R, full = N / Tc, rem = N % Tc;
+  cudaGraphExec_t g_full = nullptr, g_rem = nullptr;
+  uint64_t k_full = 0, k_rem = 0;
+  if (full > 0 && (st = capture(Tc, &g_full, &k_full))) return st;
+  if (rem > 0 && (st = capture(rem, &g_rem, &k_rem))) {
+    if (g_full) cudaGraphExecDestroy(g_full);
+    return st;
+  }
+  cudaError_t le = cudaSuccess;
+  for (int c = 0; c < full && le == cudaSuccess; ++c) le = cudaGraphLaunch(g_full, stream);
+  if (rem > 0 && le == cudaSuccess) le = cudaGraphLaunch(g_rem, stream);
+  if (g_full) cudaGraphExecDestroy(g_full);
+  if (g_rem) cudaGraphExecDestroy(g_rem);
+  if (le != cudaSuccess) {
+    set_error("graph launch failed: %s", cudaGetErrorString(le));
+    return GDN_ERR_CUDA;
+  }
+  count_launches(uint64_t(full) * k_full + k_rem);
+
+  yee_copy_out<T><<<eblocks, 256, 0, stream>>>(
+      d, static_cast<T*>(b->ex), static_cast<T*>(b->ey), static_cast<T*>(b->ez),
+      static_cast<T*>(b->hx), static_cast<T*>(b->hy), static_cast<T*>(b->hz));
+  for (const Mon3& m : mons) {
+    const long long cnt = m.count * p->n_freq;
+    const int blocks = int(std::min<long long>(div_up(cnt, 256), 148 * 8));
+    if (f64acc)
+      yee_dft_scale<double2><<<blocks, 256, 0, stream>>>(static_cast<double2*>(m.out), cnt, p->dt);
+    else
+      yee_dft_scale<float2><<<blocks, 256, 0, stream>>>(static_cast<float2*>(m.out), cnt, p->dt);
+  }
+  if (p->record_energy && N > 0)
+    yee_energy_finish<T><<<unsigned(div_up(N, 256)), 256, 0, stream>>>(
+        eacc, static_cast<T*>(b->out_energy), N, p->dx * p->dy * p->dz, p->mu0);
+  count_launches(1 + mons.size() + (p->record_energy && N > 0 ? 1 : 0));
+  GDN_TRY_CUDA(cudaGetLastError());
+  return GDN_OK;
+}
+
+}  // namespace yee3d
+}  // namespace gdn
+
+extern "C" int gdn_yee_workspace_size(const GdnYeeParams* p, const GdnYeePoints* pts, int f64,
+                                      size_t* bytes) {
+  if (!p || !bytes) {
+    gdn::set_error("null argument");
+    return GDN_ERR_BAD_ARG;
+  }
+  if (std::min({p->nx, p->ny, p->nz}) < 3 || p->npml < 0) {
+    gdn::set_error("invalid grid");
+    return GDN_ERR_BAD_ARG;
+  }
+  if (p->n_freq > 0 && p->n_monitors > 0 && (!pts || !pts->monitors)) {
+    gdn::set_error("monitor list is null");
+    return GDN_ERR_BAD_ARG;
+  }
+  *bytes = gdn::yee3d::make_layout3(p, pts, f64 ? sizeof(double) : sizeof(float)).total;
+  return GDN_OK;
+}
+
+extern "C" int gdn_yee_run_f32(const GdnYeeParams* p, const GdnYeePoints* pts,
+                               const GdnYeeBuffers* b, void* stream) {
+  return gdn::yee3d::run3<float>(p, pts, b, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int gdn_yee_run_f64(const GdnYeeParams* p, const GdnYeePoints* pts,
+                               const GdnYeeBuffers* b, void* stream) {
+  return gdn::yee3d::run3<double>(p, pts, b, static_cast<cudaStream_t>(stream));
+}

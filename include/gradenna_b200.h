@@ -188,6 +188,68 @@ int gdn_tm_run_noalloc_f32(const GdnTmParams* p, const GdnTmPoints* pts,
                            const GdnTmBuffers* b, void* stream);
 
 /* ------------------------------------------------------------------------ */
+/* 3D Yee                                                                   */
+/* ------------------------------------------------------------------------ */
+
+/* One 3D run (replaces SimParams3D, rust/src/lib3d.rs:40-56). Field shapes
+ * (src/gradenna/fdtd3d.py:1-13): Ex (nx-1,ny,nz), Ey (nx,ny-1,nz),
+ * Ez (nx,ny,nz-1), Hx (nx,ny-1,nz-1), Hy (nx-1,ny,nz-1), Hz (nx-1,ny-1,nz). */
+typedef struct GdnYeeParams {
+  int32_t nx, ny, nz;      /* cells per axis, >= 3 and > 2*npml + 2          */
+  int32_t npml, n_steps;
+  int32_t n_src, n_jx, n_jy;      /* Jz (Ez edges), Jx (Ex), Jy (Ey) sources  */
+  int32_t n_mx, n_my, n_mz;       /* magnetic currents on Hx, Hy, Hz          */
+  int32_t n_probes;               /* Ez probes                                */
+  int32_t has_port;               /* 1: one z-directed RVS port               */
+  int32_t n_freq, dft_f64, n_monitors;
+  int32_t record_energy, cw_sources;
+  double dt, dx, dy, dz, mu0;
+} GdnYeeParams;
+
+/* Host-memory index lists: (n, 3) int32 row-major (i, j, k) in each source's
+ * own component grid; monitors as for 2D with comp 0..5 = ex ey ez hx hy hz. */
+typedef struct GdnYeePoints {
+  const int32_t *src, *jx, *jy, *mx, *my, *mz, *probe;
+  int32_t port[3];
+  const GdnDftMonitor* monitors;
+} GdnYeePoints;
+
+/* Device buffers (field dtype float for *_f32, double for *_f64). The CPML
+ * tables are per axis a = x, y, z: E-type (sampled on the PEC interior,
+ * n_a - 2 entries) and H-type (half grid, n_a - 1 entries) 1/kappa tables and
+ * the slab b/c tables (npml entries, lo/hi), as built by axis_coefficients
+ * (src/gradenna/cpml.py:161-208) and sliced by fdtd3d.py:478-503. */
+typedef struct GdnYeeBuffers {
+  const void *ca, *cb, *eps;              /* (nx, ny, nz) node values          */
+  const void *ik_e[3], *ik_h[3];
+  const void *b_e_lo[3], *c_e_lo[3], *b_e_hi[3], *c_e_hi[3];
+  const void *b_h_lo[3], *c_h_lo[3], *b_h_hi[3], *c_h_hi[3];
+  double dt_mu, inv_dx, inv_dy, inv_dz;
+  double a_port, b_port, c_port;          /* semi-implicit RVS (fdtd3d.py:517-525) */
+  const void *cb_src, *cb_jx, *cb_jy;     /* per source                        */
+  const void *src_cur, *jx_cur, *jy_cur;  /* (n_steps, n)                      */
+  const void *mx_cur, *my_cur, *mz_cur;   /* (n_steps, n)                      */
+  const void *port_vs;                    /* (n_steps)                         */
+  const double *cw_env;                   /* CW mode as for 2D (complex128 W)  */
+  const double *src_w, *jx_w, *jy_w, *mx_w, *my_w, *mz_w;
+  const double *ph_e, *ph_h;              /* complex128 (n_steps, n_freq)      */
+  void *ex, *ey, *ez, *hx, *hy, *hz;      /* final fields                      */
+  void *out_probe, *out_v, *out_i, *out_energy;
+  void *dft[6];                           /* full-grid DFT when n_monitors = 0 */
+  void *workspace;
+  size_t workspace_bytes;
+} GdnYeeBuffers;
+
+int gdn_yee_workspace_size(const GdnYeeParams* p, const GdnYeePoints* pts, int f64, size_t* bytes);
+
+/* Run the whole 3D time loop (replaces gradenna_3d_run_f32/_f64,
+ * rust/src/lib3d.rs:191-828; step semantics of fdtd3d.py:559-679). */
+int gdn_yee_run_f32(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuffers* b,
+                    void* stream);
+int gdn_yee_run_f64(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuffers* b,
+                    void* stream);
+
+/* ------------------------------------------------------------------------ */
 /* Objective reductions and the frequency-domain adjoint contraction (2D)   */
 /* ------------------------------------------------------------------------ */
 
