@@ -259,3 +259,24 @@ def simulate_3d(grid: Grid3D, *, eps_r=1.0, sigma=0.0, source_ijk=None, source_c
 
     return SimResult3D(probe_out, v_out if has_port else None, i_out if has_port else None,
                        energy, acc if has_dft else None, ex, ey, ez, hx, hy, hz)
+
+
+def time_series_dft(x, dt, freqs, t0=0.0):
+    """fdtd3d.py:186-197."""
+    x = np.asarray(x, np.float64)
+    f = np.atleast_1d(np.asarray(freqs, np.float64))
+    t = t0 + dt * np.arange(x.shape[0])
+    return dt * np.tensordot(np.exp(-2j * np.pi * f[:, None] * t[None, :]), x, axes=1)
+
+
+def port_impedance(res, grid, freqs, deembed_gap=True, eps_r_port=1.0):
+    """fdtd3d.py:200-243."""
+    dt = grid.dt
+    v = time_series_dft(res.port_v, dt, freqs, 0.5 * dt)
+    i = time_series_dft(res.port_i, dt, freqs, 0.5 * dt)
+    if not deembed_gap:
+        return v / i
+    f = np.atleast_1d(np.asarray(freqs, np.float64))
+    omega_d = 2.0 * np.tan(np.pi * f * dt) / dt
+    c_gap = EPS0 * eps_r_port * grid.dx * grid.dy / grid.dz
+    return 1.0 / (i / v + 1j * omega_d * c_gap)
