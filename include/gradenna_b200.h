@@ -284,6 +284,48 @@ int gdn_tm_adjoint_contract(int32_t n_cells, int32_t n_freq, double dt, double k
                             const double* sigma, const void* z, double* grad_sigma,
                             double* grad_eps_r, void* stream);
 
+/* ------------------------------------------------------------------------ */
+/* Near-to-far-field projection (3D and 2D)                                 */
+/* ------------------------------------------------------------------------ */
+
+/* Radiation vectors and far-field pattern amplitudes of equivalent surface
+ * currents (replaces the einsum core of ntff_3d, src/gradenna/ntff.py:399-428):
+ *   N_d = sum_p w_p exp(+i k rhat_d . r_p) J_p,  L_d likewise with M_p,
+ *   E_theta = -(i k / 4 pi)(L_phi + eta0 N_theta),
+ *   E_phi   = +(i k / 4 pi)(L_theta - eta0 N_phi).
+ * DEVICE arrays, complex128 when c128 = 1 else complex64 for J, M, out:
+ *   pos (n_pts, 3) double, w (n_pts) double, J/M (n_freq, n_pts, 3),
+ *   k (n_freq) double, dirs (n_dir, 4) double = (cos th, sin th, cos ph, sin ph),
+ *   out (n_freq, n_dir, 2) = (E_theta, E_phi). */
+int gdn_ntff3d_project(int32_t n_freq, int32_t n_pts, int32_t n_dir, int32_t c128,
+                       const double* pos, const double* w, const void* J, const void* M,
+                       const double* k, const double* dirs, double eta0, void* out,
+                       void* stream);
+
+/* Adjoint of gdn_ntff3d_project: given g_out (n_freq, n_dir, 2) in torch's
+ * complex-gradient convention, WRITES g_J, g_M (n_freq, n_pts, 3). */
+int gdn_ntff3d_project_grad(int32_t n_freq, int32_t n_pts, int32_t n_dir, int32_t c128,
+                            const double* pos, const double* w, const double* k,
+                            const double* dirs, double eta0, const void* g_out, void* g_J,
+                            void* g_M, void* stream);
+
+/* 2D contour projection (ntff_2d, src/gradenna/ntff.py:213-228):
+ *   E_far(f, phi) = pref_f sum_p w_p (eta0 Jz_p - (n_p . u_phi) Ez_p)
+ *                   exp(+i k (x_p cos phi + y_p sin phi)),
+ * pref_f = -sqrt(i k / 8 pi). pos (n_pts, 4) double = (x, y, n_x, n_y);
+ * Jz, Ez (n_freq, n_pts); angles (n_ang) double; out (n_freq, n_ang). */
+int gdn_ntff2d_project(int32_t n_freq, int32_t n_pts, int32_t n_ang, int32_t c128,
+                       const double* pos, const double* w, const void* Jz, const void* Ez,
+                       const double* k, const double* angles, double eta0, void* out,
+                       void* stream);
+
+/* Adjoint of gdn_ntff2d_project: given g_out (n_freq, n_ang) in torch's
+ * complex-gradient convention, WRITES g_Jz, g_Ez (n_freq, n_pts). */
+int gdn_ntff2d_project_grad(int32_t n_freq, int32_t n_pts, int32_t n_ang, int32_t c128,
+                            const double* pos, const double* w, const double* k,
+                            const double* angles, double eta0, const void* g_out, void* g_Jz,
+                            void* g_Ez, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
