@@ -91,6 +91,8 @@ def _configure(lib) -> None:
     lib.gdn_last_error.argtypes = []
     lib.gdn_kernel_launches.restype = ctypes.c_uint64
     lib.gdn_kernel_launches.argtypes = []
+    lib.gdn_tm_loop_stats.restype = ctypes.c_int
+    lib.gdn_tm_loop_stats.argtypes = [P_f64, P_f64, ctypes.POINTER(ctypes.c_int64), c_int32]
     lib.gdn_tm_workspace_size.restype = ctypes.c_int
     lib.gdn_tm_workspace_size.argtypes = [
         ctypes.POINTER(TmParams), ctypes.POINTER(TmPoints), ctypes.c_int,
@@ -170,3 +172,14 @@ def ptr(t) -> int | None:
 def kernel_launches() -> int:
     """Kernels this library has launched in this process (gdn_kernel_launches)."""
     return int(load().gdn_kernel_launches())
+
+
+def tm_loop_stats(reset: bool = True):
+    """(ms, cell_steps, blocks) of the 2D time loops since the last reset
+    (gdn_tm_loop_stats): device time between events recorded on the run's
+    stream around each time loop."""
+    ms, cs = ctypes.c_double(), ctypes.c_double()
+    nb = ctypes.c_int64()
+    check(load().gdn_tm_loop_stats(ctypes.byref(ms), ctypes.byref(cs), ctypes.byref(nb),
+                                   int(reset)))
+    return ms.value, cs.value, nb.value

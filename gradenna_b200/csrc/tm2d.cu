@@ -20,10 +20,12 @@
 //   * Field state is a ping-pong pair of padded planes (ghost rows/columns
 //     stay zero: they are also the PEC ring); launch k reads pair k&1 and
 //     writes pair (k+1)&1, so halo reads never race with owners' writes.
-//   * CPML psi lives in slab storage in HBM (double-buffered by launch
-//     parity). PML tiles copy the psi of their whole extended region into a
-//     private HBM buffer, advance it across the sub-steps and write back the
-//     owned cells, so halo recomputation never touches shared state.
+//   * Two tile classes run as two concurrent launches per block: interior
+//     tiles (no CPML, no PEC ring: five staged planes, branch-free vector
+//     sweeps) and general tiles, which also stage the four CPML psi planes
+//     (ezx, ezy, hyx, hxy: padded planes, zero outside the slabs, ping-pong
+//     by launch parity like the fields) and use per-row/column coefficient
+//     and mask tables so their sweeps are branch-free too.
 //   * Point work (sources, ports, probes, magnetic currents) is binned on the
 //     host into per-tile lists that include the halo; injections are applied
 //     to every copy of a cell, records (V, I, probes) only by the owner.
@@ -38,6 +40,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <mutex>
+#include <vector>
 
 #include "common.cuh"
 
@@ -1149,6 +1152,51 @@ static int finalize(const GdnTmParams* p, const GdnTmBuffers* b, const Run<T>& R
   return GDN_OK;
 }
 
+// Time-loop timing for gdn_tm_loop_stats: events recorded on the caller's
+// stream around the replay of the time loop of every run, resolved lazily.
+struct LoopRecord {
+  cudaEvent_t a, b;
+  double cell_steps;
+  int64_t blocks;
+};
+static std::mutex g_loop_mu;
+static std::vector<LoopRecord> g_loops;
+constexpr size_t kMaxLoopRecords = 4096;
+
+struct LoopTimer {
+  cudaEvent_t a = nullptr, b = nullptr;
+  cudaStream_t s;
+  double cells;
+  int64_t blocks;
+  LoopTimer(cudaStream_t s_, double c, int64_t n) : s(s_), cells(c), blocks(n) {
+    {
+      std::lock_guard<std::mutex> lk(g_loop_mu);
+      if (g_loops.size() >= kMaxLoopRecords) return;
+    }
+    if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess ||
+        cudaEventRecord(a, s) != cudaSuccess) {
+      release();
+      cudaGetLastError();
+    }
+  }
+  void release() {
+    if (a) cudaEventDestroy(a);
+    if (b) cudaEventDestroy(b);
+    a = b = nullptr;
+  }
+  void stop(bool ok) {
+    if (!a || !b) return;
+    if (!ok || cudaEventRecord(b, s) != cudaSuccess) {
+      release();
+      return;
+    }
+    std::lock_guard<std::mutex> lk(g_loop_mu);
+    g_loops.push_back({a, b, cells, blocks});
+    a = b = nullptr;
+  }
+  ~LoopTimer() { release(); }
+};
+
 template <typename T>
 static int run(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuffers* b,
                cudaStream_t stream) {
@@ -1224,8 +1272,12 @@ static int run(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuffers*
     k_rem = per_chunk;
   }
   cudaError_t le = cudaSuccess;
+  const int tbd = R.L.cfg.tb;
+  LoopTimer timer(stream, double(p->nx) * p->ny * N,
+                  int64_t(full) * div_up(Tc, tbd) + div_up(rem, tbd));
   for (int c = 0; c < full && le == cudaSuccess; ++c) le = cudaGraphLaunch(g_full, stream);
   if (rem > 0 && le == cudaSuccess) le = cudaGraphLaunch(g_rem, stream);
+  timer.stop(le == cudaSuccess);
   if (g_full) cudaGraphExecDestroy(g_full);
   if (g_rem) cudaGraphExecDestroy(g_rem);
   if (le != cudaSuccess) {
@@ -1238,6 +1290,32 @@ static int run(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuffers*
 
 }  // namespace tm2d
 }  // namespace gdn
+
+extern "C" int gdn_tm_loop_stats(double* loop_ms, double* cell_steps, int64_t* blocks,
+                                 int32_t reset) {
+  std::lock_guard<std::mutex> lk(gdn::tm2d::g_loop_mu);
+  double ms = 0.0, cs = 0.0;
+  int64_t nb = 0;
+  for (auto& r : gdn::tm2d::g_loops) {
+    GDN_TRY_CUDA(cudaEventSynchronize(r.b));
+    float t = 0.f;
+    GDN_TRY_CUDA(cudaEventElapsedTime(&t, r.a, r.b));
+    ms += t;
+    cs += r.cell_steps;
+    nb += r.blocks;
+  }
+  if (loop_ms) *loop_ms = ms;
+  if (cell_steps) *cell_steps = cs;
+  if (blocks) *blocks = nb;
+  if (reset) {
+    for (auto& r : gdn::tm2d::g_loops) {
+      cudaEventDestroy(r.a);
+      cudaEventDestroy(r.b);
+    }
+    gdn::tm2d::g_loops.clear();
+  }
+  return GDN_OK;
+}
 
 extern "C" int gdn_tm_workspace_size(const GdnTmParams* p, const GdnTmPoints* pts, int f64,
                                      size_t* bytes) {

@@ -8,7 +8,7 @@
  *   ------------------------------------------------------------------------
  *   gradenna_tm_run_f32 / _f64                    gdn_tm_run_f32 / _f64
  *     (rust/src/lib.rs:89-142, bound in src/gradenna/native.py:140-170)
- *   gradenna_3d_run_f32 / _f64                    gdn_3d_run_f32 / _f64
+ *   gradenna_3d_run_f32 / _f64                    gdn_yee_run_f32 / _f64
  *     (rust/src/lib3d.rs:191-230, bound in src/gradenna/native3d.py:145-163)
  *   simulate_tm_native / simulate_3d_native       the Python shim
  *     (src/gradenna/native.py:200, native3d.py:174) gradenna_b200.simulate_tm
@@ -63,6 +63,17 @@ const char* gdn_last_error(void);
  * (graph replays count every kernel node they run). No reference
  * counterpart: it lets callers and benchmarks attribute device work. */
 uint64_t gdn_kernel_launches(void);
+
+/* Device time of the 2D time loops run since the last reset. Every
+ * gdn_tm_run_f32/f64 records CUDA events on its stream around the replay of
+ * its time loop (the TB-step block launches, DFT folds and step-counter
+ * advances); this call waits for those events and returns the summed
+ * milliseconds, the summed nx*ny*n_steps and the number of blocks (one
+ * block = one TB-step launch of the whole grid), then forgets the records
+ * when reset != 0. At most 4096 runs are recorded between resets. No
+ * reference counterpart: it gives benchmarks a per-launch kernel time
+ * measured inside their own timed region. */
+int gdn_tm_loop_stats(double* loop_ms, double* cell_steps, int64_t* blocks, int32_t reset);
 
 /* ------------------------------------------------------------------------ */
 /* 2D TM                                                                    */
