@@ -37,6 +37,7 @@
 //     captured once as a CUDA graph and replayed; kernels read the absolute
 //     step index from a device counter.
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdlib>
 #include <mutex>
@@ -75,6 +76,16 @@ struct MonD {
   void* out;
 };
 
+// One monitor's part inside one tile: cells [a0, a1) x [b0, b1) of
+// component comp, written to ring index base + i * w + j. Binned per tile on
+// the host so a tile touches only the monitors that cross it.
+struct MonW {
+  int a0, a1, b0, b1, comp, w;
+  long long base;
+};
+constexpr int MAXW = 16;  // per-tile monitor parts staged in shared memory
+constexpr int MAXF = 64;  // monitors whose offsets the fold stages in shared memory
+
 template <typename T>
 struct Dev {
   int nx, ny, ld, npml, n_steps, n_freq, R, tiles_x;
@@ -84,6 +95,8 @@ struct Dev {
   long long mon_cells;
   int n_mons;
   const MonD* mons;
+  const int* mw_off;  // per-tile CSR over mw
+  const MonW* mw;
   const T *ca, *cb, *eps;  // ca/cb padded planes; eps caller (nx, ny)
   const T *ikx_e, *iky_e, *ikx_h, *iky_h;
   const T *b_ezx_lo, *c_ezx_lo, *b_ezx_hi, *c_ezx_hi;
@@ -295,6 +308,13 @@ __global__ void __launch_bounds__(NT) tm_tb(Dev<T> d, const int* tiles, int sub0
     const int m = d.port_pts[tl.pb + k].m;
     sPv[k * TB + s] = d.cb_vs[m] * d.port_vs[(long long)(n0 + s) * d.n_ports + m];
   }
+  __shared__ MonW sMW[MAXW];
+  int wb = 0, nw = 0;
+  if (d.n_mons > 0) {
+    wb = d.mw_off[tile];
+    nw = d.mw_off[tile + 1] - wb;
+    for (int q = tid; q < min(nw, MAXW); q += NT) sMW[q] = d.mw[wb + q];
+  }
   cp_async_wait_all();
   __syncthreads();
   const T dt_mu = d.dt_mu, inv_dx = d.inv_dx, inv_dy = d.inv_dy;
@@ -425,19 +445,20 @@ __global__ void __launch_bounds__(NT) tm_tb(Dev<T> d, const int* tiles, int sub0
       const Pt pt = d.probe_pts[q];
       d.out_probe[(long long)n * d.n_probes + pt.m] = sEz[(pt.i - ie) * EW + (pt.j - je)];
     }
-    // Monitored cells of the owned tile into ring slot n % R.
-    if (d.n_mons > 0) {
+    // Monitored cells of the owned tile into ring slot n % R: only the
+    // monitor parts binned to this tile; one warp per row, lanes along it.
+    if (nw > 0) {
+      constexpr int NW = NT / 32;
+      const int warp = tid >> 5, lane = tid & 31;
       T* slot = d.mring + (long long)(n % d.R) * d.mon_cells;
-      for (int mm = 0; mm < d.n_mons; ++mm) {
-        const MonD mo = d.mons[mm];
-        const int a0 = max(mo.lo0, i0), a1 = min(mo.lo0 + mo.h, i0 + TI);
-        const int b0 = max(mo.lo1, j0), b1 = min(mo.lo1 + mo.w, j0 + TJ);
-        if (a0 >= a1 || b0 >= b1) continue;
-        const T* f = mo.comp == 0 ? sEz : (mo.comp == 1 ? sHx : sHy);
-        const int bw = b1 - b0;
-        for (int q = tid; q < (a1 - a0) * bw; q += NT) {
-          const int i = a0 + q / bw, j = b0 + q % bw;
-          slot[mo.off + (long long)(i - mo.lo0) * mo.w + (j - mo.lo1)] = f[(i - ie) * EW + (j - je)];
+      for (int q = 0; q < nw; ++q) {
+        const MonW e = q < MAXW ? sMW[q] : d.mw[wb + q];
+        const T* f = (e.comp == 0 ? sEz : (e.comp == 1 ? sHx : sHy)) - je;
+        T* o = slot + e.base;
+        for (int i = e.a0 + warp; i < e.a1; i += NW) {
+          const T* fr = f + (i - ie) * EW;
+          T* orow = o + (long long)i * e.w;
+          for (int j = e.b0 + lane; j < e.b1; j += 32) orow[j] = fr[j];
         }
       }
     }
@@ -485,15 +506,31 @@ __global__ void __launch_bounds__(256) tm_dft_fold(Dev<T> d, int sub0, int cnt) 
     sph[2 * (cnt * K + idx)] = A(ph.x);
     sph[2 * (cnt * K + idx) + 1] = A(ph.y);
   }
+  // Ring cells of all monitors form one index space (monitor m holds
+  // [off_m, off_m + count_m)); each thread finds its monitor by binary search.
+  __shared__ long long sOff[MAXF];
+  const int nm = d.n_mons;
+  if (nm <= MAXF)
+    for (int m = threadIdx.x; m < nm; m += blockDim.x) sOff[m] = d.mons[m].off;
   __syncthreads();
-  const MonD mon = d.mons[blockIdx.y];
   const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= mon.count) return;
+  if (r >= d.mon_cells) return;
+  int lo = 0, hi = nm - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    const long long o = nm <= MAXF ? sOff[mid] : d.mons[mid].off;
+    if (o <= r)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  const MonD mon = d.mons[lo];
+  const long long loc = r - mon.off;
   const A* ph = sph + (mon.comp == 0 ? 0 : 2 * cnt * K);
   A are[KM], aim[KM];
 #pragma unroll
   for (int k = 0; k < KM; ++k) are[k] = aim[k] = A(0);
-  const T* base = d.mring + mon.off + r;
+  const T* base = d.mring + r;
 #pragma unroll 4
   for (int t = 0; t < cnt; ++t) {
     const A x = A(base[(long long)((n0 + t) % d.R) * d.mon_cells]);
@@ -505,7 +542,7 @@ __global__ void __launch_bounds__(256) tm_dft_fold(Dev<T> d, int sub0, int cnt) 
       }
     }
   }
-  C* acc = static_cast<C*>(mon.out) + r;
+  C* acc = static_cast<C*>(mon.out) + loc;
 #pragma unroll
   for (int k = 0; k < KM; ++k) {
     if (k < K) {
@@ -613,9 +650,9 @@ __global__ void tm_dft_scale(C* a, long long count, double s) {
 struct Layout {
   Cfg cfg;
   int ld = 0, rows = 0, tiles_x = 0, tiles_y = 0, n_tiles = 0, R = 32, n_gen = 0, n_int = 0;
-  long long plane = 0, mon_cells = 0;
-  size_t state[2], ca, cb, psi[2], zero_end, tile_list, off[5], pts[5], mons, mring, step,
-      eacc, total;
+  long long plane = 0, mon_cells = 0, n_mw = 0;
+  size_t state[2], ca, cb, psi[2], zero_end, tile_list, off[5], pts[5], mons, mw_off, mw, mring,
+      step, eacc, total;
 };
 
 // Tile shape: one step per launch when the energy is recorded, else the
@@ -632,17 +669,39 @@ static Cfg pick_cfg(const GdnTmParams* p, size_t esize) {
   return big >= 148 ? c[0] : c[2];
 }
 
-static long long monitor_cells(const GdnTmParams* p, const GdnTmPoints* pts) {
-  if (p->n_freq <= 0) return 0;
-  if (p->n_monitors == 0)
-    return (long long)p->nx * p->ny + (long long)p->nx * (p->ny - 1) +
-           (long long)(p->nx - 1) * p->ny;
-  long long c = 0;
+// Monitor boxes {comp, lo0, lo1, h, w} in ring order: the listed boxes, or
+// the three full components when none are listed.
+static std::vector<std::array<int, 5>> monitor_boxes(const GdnTmParams* p,
+                                                     const GdnTmPoints* pts) {
+  std::vector<std::array<int, 5>> v;
+  if (p->n_freq <= 0) return v;
+  if (p->n_monitors == 0) {
+    v.push_back({0, 0, 0, p->nx, p->ny});
+    v.push_back({1, 0, 0, p->nx, p->ny - 1});
+    v.push_back({2, 0, 0, p->nx - 1, p->ny});
+    return v;
+  }
   for (int k = 0; k < p->n_monitors; ++k) {
     const GdnDftMonitor& m = pts->monitors[k];
-    c += (long long)(m.hi[0] - m.lo[0]) * (m.hi[1] - m.lo[1]);
+    v.push_back({m.comp, m.lo[0], m.lo[1], m.hi[0] - m.lo[0], m.hi[1] - m.lo[1]});
   }
+  return v;
+}
+
+static long long monitor_cells(const GdnTmParams* p, const GdnTmPoints* pts) {
+  long long c = 0;
+  for (const auto& b : monitor_boxes(p, pts)) c += (long long)b[3] * b[4];
   return c;
+}
+
+// Number of (tile, monitor) parts: every tile a monitor box crosses.
+static long long monitor_parts(const GdnTmParams* p, const GdnTmPoints* pts, const Cfg& c) {
+  long long n = 0;
+  for (const auto& b : monitor_boxes(p, pts))
+    if (b[3] > 0 && b[4] > 0)
+      n += (long long)((b[1] + b[3] - 1) / c.ti - b[1] / c.ti + 1) *
+           ((b[2] + b[4] - 1) / c.tj - b[2] / c.tj + 1);
+  return n;
 }
 
 // Interior tiles: every cell of the extended region is an interior Ez cell
@@ -669,6 +728,7 @@ static Layout make_layout(const GdnTmParams* p, const GdnTmPoints* pts, size_t e
   L.rows = L.tiles_y * c.ti + 2 * PADI;
   L.plane = (long long)L.rows * L.ld;
   L.mon_cells = pts ? monitor_cells(p, pts) : 0;
+  L.n_mw = pts ? monitor_parts(p, pts, c) : 0;
   if (ring_steps > 0) {
     L.R = ring_steps;
   } else {
@@ -700,6 +760,8 @@ static Layout make_layout(const GdnTmParams* p, const GdnTmPoints* pts, size_t e
     L.pts[k] = cv.take<Pt>(4 * size_t(std::max(counts[k], 1)));
   }
   L.mons = cv.take<MonD>(size_t(std::max(p->n_monitors, 3)));
+  L.mw_off = cv.take<int>(L.n_tiles + 1);
+  L.mw = cv.take<MonW>(size_t(std::max<long long>(L.n_mw, 1)));
   L.mring = cv.take<char>(std::max<size_t>(size_t(L.mon_cells) * L.R, 1) * esize);
   L.eacc = cv.take<double>(p->record_energy ? 2 * size_t(std::max(p->n_steps, 1)) : 1);
   L.total = cv.bytes();
@@ -936,7 +998,7 @@ static uint64_t launch_tb(const Run<T>& R, int sub0, int nsub, cudaStream_t s, c
 
 template <typename T, typename A>
 static void launch_fold(const Run<T>& R, int cnt, int K, cudaStream_t s) {
-  const dim3 dg(unsigned(div_up(R.max_cells, 256)), unsigned(R.mons.size()));
+  const unsigned dg = unsigned(div_up(R.L.mon_cells, 256));
   const size_t sm = size_t(4) * cnt * K * sizeof(A);
   if (K <= 4)
     tm_dft_fold<T, A, 4><<<dg, 256, sm, s>>>(R.d, 0, cnt);
@@ -1080,27 +1142,56 @@ static int prepare(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuff
   const bool f64acc = p->dft_f64 != 0;
   const size_t csz = f64acc ? sizeof(double2) : sizeof(float2);
   R.mons.clear();
-  if (p->n_freq > 0) {
+  {
+    void* const full_out[3] = {b->dft_ez, b->dft_hx, b->dft_hy};
     long long off = 0;
-    if (p->n_monitors == 0) {
-      void* const outs[3] = {b->dft_ez, b->dft_hx, b->dft_hy};
-      const int shp[3][2] = {{nx, ny}, {nx, ny - 1}, {nx - 1, ny}};
-      for (int c = 0; c < 3; ++c) {
-        const long long cnt = (long long)shp[c][0] * shp[c][1];
-        R.mons.push_back(MonD{c, 0, 0, shp[c][0], shp[c][1], 0, cnt, off, outs[c]});
-        off += cnt;
-      }
-    } else {
-      for (int k = 0; k < p->n_monitors; ++k) {
-        const GdnDftMonitor& m = pts->monitors[k];
-        const int h = m.hi[0] - m.lo[0], w = m.hi[1] - m.lo[1];
-        R.mons.push_back(MonD{m.comp, m.lo[0], m.lo[1], h, w, 0, (long long)h * w, off, m.out});
-        off += (long long)h * w;
-      }
+    int k = 0;
+    for (const auto& bx : monitor_boxes(p, pts)) {
+      void* out = p->n_monitors == 0 ? full_out[k] : pts->monitors[k].out;
+      const long long cnt = (long long)bx[3] * bx[4];
+      R.mons.push_back(MonD{bx[0], bx[1], bx[2], bx[3], bx[4], 0, cnt, off, out});
+      off += cnt;
+      ++k;
     }
   }
   d.n_mons = int(R.mons.size());
   d.mons = reinterpret_cast<const MonD*>(ws + L.mons);
+  // Monitor parts per tile (CSR), in tile order.
+  {
+    const Cfg& c = L.cfg;
+    std::vector<std::vector<MonW>> per(L.n_tiles);
+    for (const MonD& m : R.mons) {
+      if (m.h <= 0 || m.w <= 0) continue;
+      for (int ty = m.lo0 / c.ti; ty <= (m.lo0 + m.h - 1) / c.ti; ++ty)
+        for (int tx = m.lo1 / c.tj; tx <= (m.lo1 + m.w - 1) / c.tj; ++tx) {
+          MonW e;
+          e.a0 = std::max(m.lo0, ty * c.ti);
+          e.a1 = std::min(m.lo0 + m.h, (ty + 1) * c.ti);
+          e.b0 = std::max(m.lo1, tx * c.tj);
+          e.b1 = std::min(m.lo1 + m.w, (tx + 1) * c.tj);
+          e.comp = m.comp;
+          e.w = m.w;
+          e.base = m.off - (long long)m.lo0 * m.w - m.lo1;
+          per[ty * L.tiles_x + tx].push_back(e);
+        }
+    }
+    std::vector<int> moff(L.n_tiles + 1, 0);
+    std::vector<MonW> mw;
+    mw.reserve(size_t(L.n_mw));
+    for (int t = 0; t < L.n_tiles; ++t) {
+      mw.insert(mw.end(), per[t].begin(), per[t].end());
+      moff[t + 1] = int(mw.size());
+    }
+    if ((long long)mw.size() != L.n_mw)
+      GDN_BAD_ARG("internal: %zu monitor parts, layout sized for %lld", mw.size(), L.n_mw);
+    GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.mw_off, moff.data(), moff.size() * sizeof(int),
+                                 cudaMemcpyHostToDevice, stream));
+    if (!mw.empty())
+      GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.mw, mw.data(), mw.size() * sizeof(MonW),
+                                   cudaMemcpyHostToDevice, stream));
+    d.mw_off = reinterpret_cast<const int*>(ws + L.mw_off);
+    d.mw = reinterpret_cast<const MonW*>(ws + L.mw);
+  }
   R.max_cells = 0;
   for (const MonD& m : R.mons) {
     R.max_cells = std::max(R.max_cells, m.count);
