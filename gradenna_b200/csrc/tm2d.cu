@@ -153,19 +153,87 @@ struct TileLists {
   int mb, me, yb, ye, sb, se, pb, pe, qb, qe;
 };
 
-template <typename T, int EW, int NT>
+// Point-source values of a launch are staged once in shared memory (sVal):
+// item (k * TB + s) is the k-th record of the tile's Jz list at sub-step s,
+// then the Mx list, then the My list; items past MAXV are computed in place.
+template <typename T>
+struct Vals {
+  static constexpr int MAXV = 4096 / int(sizeof(T));
+};
+
+template <typename T>
+__device__ __forceinline__ T src_term(const Dev<T>& d, int m, int n) {
+  return d.cb_src[m] * point_value(d, d.src_cur, d.src_w, d.ph_e, d.n_src, m, n);
+}
+template <typename T>
+__device__ __forceinline__ T mx_term(const Dev<T>& d, int m, int n) {
+  return d.dt_mu * point_value(d, d.mx_cur, d.mx_w, d.ph_h, d.n_mx, m, n);
+}
+template <typename T>
+__device__ __forceinline__ T my_term(const Dev<T>& d, int m, int n) {
+  return d.dt_mu * point_value(d, d.my_cur, d.my_w, d.ph_h, d.n_my, m, n);
+}
+
+template <typename T, int TB, int NT>
+__device__ __forceinline__ void stage_values(const Dev<T>& d, const TileLists& L, T* sVal,
+                                             int n0, int nsub, int tid) {
+  constexpr int MAXV = Vals<T>::MAXV;
+  const int nj = (L.se - L.sb) * TB, nxm = (L.me - L.mb) * TB, nym = (L.ye - L.yb) * TB;
+  const int tot = min(nj + nxm + nym, MAXV);
+  for (int q = tid; q < tot; q += NT) {
+    const int s = q % TB;
+    if (s >= nsub) continue;
+    if (q < nj) {
+      sVal[q] = src_term(d, d.src_pts[L.sb + q / TB].m, n0 + s);
+    } else if (q < nj + nxm) {
+      sVal[q] = mx_term(d, d.mx_pts[L.mb + (q - nj) / TB].m, n0 + s);
+    } else {
+      sVal[q] = my_term(d, d.my_pts[L.yb + (q - nj - nxm) / TB].m, n0 + s);
+    }
+  }
+}
+
+template <typename T, int TB, int EW, int NT>
 __device__ __forceinline__ void apply_magnetic(const Dev<T>& d, const TileLists& L, T* sHx,
-                                               T* sHy, int ie, int je, int n, int tid) {
+                                               T* sHy, const T* sVal, int ie, int je, int n,
+                                               int s, int tid) {
+  constexpr int MAXV = Vals<T>::MAXV;
+  const int nj = (L.se - L.sb) * TB, nxm = (L.me - L.mb) * TB;
   for (int q = L.mb + tid; q < L.me; q += NT) {
     const Pt pt = d.mx_pts[q];
-    atomicAdd(&sHx[(pt.i - ie) * EW + (pt.j - je)],
-              -(d.dt_mu * point_value(d, d.mx_cur, d.mx_w, d.ph_h, d.n_mx, pt.m, n)));
+    const int v = nj + (q - L.mb) * TB + s;
+    atomicAdd(&sHx[(pt.i - ie) * EW + (pt.j - je)], -(v < MAXV ? sVal[v] : mx_term(d, pt.m, n)));
   }
   for (int q = L.yb + tid; q < L.ye; q += NT) {
     const Pt pt = d.my_pts[q];
-    atomicAdd(&sHy[(pt.i - ie) * EW + (pt.j - je)],
-              -(d.dt_mu * point_value(d, d.my_cur, d.my_w, d.ph_h, d.n_my, pt.m, n)));
+    const int v = nj + nxm + (q - L.yb) * TB + s;
+    atomicAdd(&sHy[(pt.i - ie) * EW + (pt.j - je)], -(v < MAXV ? sVal[v] : my_term(d, pt.m, n)));
   }
+}
+
+// Monitored cells of the tile for the Ez monitors (want_e) or the Hx/Hy
+// monitors (!want_e) into ring slot n % R: only the monitor parts binned to
+// this tile; one warp per row, lanes along it.
+template <typename T, int EW, int NT>
+__device__ __forceinline__ void write_ring(const Dev<T>& d, const MonW* sMW, int wb, int nw,
+                                           bool want_e, const T* sEz, const T* sHx,
+                                           const T* sHy, int ie, int je, int n, int tid) {
+  constexpr int NW = NT / 32;
+  const int warp = tid >> 5, lane = tid & 31;
+  T* slot = d.mring + (long long)(n % d.R) * d.mon_cells;
+  auto part = [&](const MonW& e) {
+    if ((e.comp == 0) != want_e) return;
+    const T* f = (e.comp == 0 ? sEz : (e.comp == 1 ? sHx : sHy)) - je;
+    T* o = slot + e.base;
+    for (int i = e.a0 + warp; i < e.a1; i += NW) {
+      const T* fr = f + (i - ie) * EW;
+      T* orow = o + (long long)i * e.w;
+      for (int j = e.b0 + lane; j < e.b1; j += 32) orow[j] = fr[j];
+    }
+  };
+  const int ns = min(nw, MAXW);
+  for (int q = 0; q < ns; ++q) part(sMW[q]);
+  for (int q = MAXW; q < nw; ++q) part(d.mw[wb + q]);
 }
 
 // Per-row / per-column CPML coefficients and validity masks of a general
@@ -315,6 +383,8 @@ __global__ void __launch_bounds__(NT) tm_tb(Dev<T> d, const int* tiles, int sub0
     nw = d.mw_off[tile + 1] - wb;
     for (int q = tid; q < min(nw, MAXW); q += NT) sMW[q] = d.mw[wb + q];
   }
+  __shared__ T sVal[Vals<T>::MAXV];
+  stage_values<T, TB, NT>(d, tl, sVal, n0, nsub, tid);
   cp_async_wait_all();
   __syncthreads();
   const T dt_mu = d.dt_mu, inv_dx = d.inv_dx, inv_dy = d.inv_dy;
@@ -362,9 +432,11 @@ __global__ void __launch_bounds__(NT) tm_tb(Dev<T> d, const int* tiles, int sub0
       st16(sHx + q, hx);
       st16(sHy + q, hy);
     }
+    // Ez monitors of the previous sub-step (Ez is not written in this phase).
+    if (nw > 0 && s > 0) write_ring<T, EW, NT>(d, sMW, wb, nw, true, sEz, sHx, sHy, ie, je, n - 1, tid);
     __syncthreads();
     if (tl.mb < tl.me || tl.yb < tl.ye) {
-      apply_magnetic<T, EW, NT>(d, tl, sHx, sHy, ie, je, n, tid);
+      apply_magnetic<T, TB, EW, NT>(d, tl, sHx, sHy, sVal, ie, je, n, s, tid);
       __syncthreads();
     }
     // Port current on H^{n+1/2} and the Ez^n snapshot (fdtd2d.py:430-436).
@@ -415,13 +487,16 @@ __global__ void __launch_bounds__(NT) tm_tb(Dev<T> d, const int* tiles, int sub0
       }
       st16(sEz + q, e);
     }
+    // H monitors of this sub-step (H is final and only read in this phase).
+    if (nw > 0) write_ring<T, EW, NT>(d, sMW, wb, nw, false, sEz, sHx, sHy, ie, je, n, tid);
     __syncthreads();
     // Jz line sources on every copy: Ez -= cb_src J (fdtd2d.py:444).
     if (tl.sb < tl.se) {
       for (int q = tl.sb + tid; q < tl.se; q += NT) {
         const Pt pt = d.src_pts[q];
+        const int v = (q - tl.sb) * TB + s;
         atomicAdd(&sEz[(pt.i - ie) * EW + (pt.j - je)],
-                  -(d.cb_src[pt.m] * point_value(d, d.src_cur, d.src_w, d.ph_e, d.n_src, pt.m, n)));
+                  -(v < Vals<T>::MAXV ? sVal[v] : src_term(d, pt.m, n)));
       }
       __syncthreads();
     }
@@ -445,25 +520,11 @@ __global__ void __launch_bounds__(NT) tm_tb(Dev<T> d, const int* tiles, int sub0
       const Pt pt = d.probe_pts[q];
       d.out_probe[(long long)n * d.n_probes + pt.m] = sEz[(pt.i - ie) * EW + (pt.j - je)];
     }
-    // Monitored cells of the owned tile into ring slot n % R: only the
-    // monitor parts binned to this tile; one warp per row, lanes along it.
-    if (nw > 0) {
-      constexpr int NW = NT / 32;
-      const int warp = tid >> 5, lane = tid & 31;
-      T* slot = d.mring + (long long)(n % d.R) * d.mon_cells;
-      for (int q = 0; q < nw; ++q) {
-        const MonW e = q < MAXW ? sMW[q] : d.mw[wb + q];
-        const T* f = (e.comp == 0 ? sEz : (e.comp == 1 ? sHx : sHy)) - je;
-        T* o = slot + e.base;
-        for (int i = e.a0 + warp; i < e.a1; i += NW) {
-          const T* fr = f + (i - ie) * EW;
-          T* orow = o + (long long)i * e.w;
-          for (int j = e.b0 + lane; j < e.b1; j += 32) orow[j] = fr[j];
-        }
-      }
-    }
-    __syncthreads();
   }
+  // Ez monitors of the last sub-step, in the same read-only phase as the
+  // write-back below.
+  if (nw > 0 && nsub > 0)
+    write_ring<T, EW, NT>(d, sMW, wb, nw, true, sEz, sHx, sHy, ie, je, n0 + nsub - 1, tid);
 
   // ---- owned fields to the other state slot; owned psi back to the slabs ----
   constexpr int TV = TJ / V;
@@ -531,16 +592,33 @@ __global__ void __launch_bounds__(256) tm_dft_fold(Dev<T> d, int sub0, int cnt) 
 #pragma unroll
   for (int k = 0; k < KM; ++k) are[k] = aim[k] = A(0);
   const T* base = d.mring + r;
-#pragma unroll 4
-  for (int t = 0; t < cnt; ++t) {
-    const A x = A(base[(long long)((n0 + t) % d.R) * d.mon_cells]);
+  // Eight ring loads in flight per thread, then their FMAs.
+  int slot = n0 % d.R;
+  for (int t0 = 0; t0 < cnt; t0 += 8) {
+    A x[8];
 #pragma unroll
-    for (int k = 0; k < KM; ++k) {
-      if (k < K) {
-        are[k] += ph[2 * (t * K + k)] * x;
-        aim[k] += ph[2 * (t * K + k) + 1] * x;
+    for (int u = 0; u < 8; ++u) {
+      x[u] = A(0);
+      if (t0 + u < cnt) {
+        const int sl = slot + u >= d.R ? slot + u - d.R : slot + u;
+        x[u] = A(base[(long long)sl * d.mon_cells]);
       }
     }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      if (t0 + u < cnt) {
+        const A* pt = ph + 2 * (t0 + u) * K;
+#pragma unroll
+        for (int k = 0; k < KM; ++k) {
+          if (k < K) {
+            are[k] += pt[2 * k] * x[u];
+            aim[k] += pt[2 * k + 1] * x[u];
+          }
+        }
+      }
+    }
+    slot += 8;
+    if (slot >= d.R) slot -= d.R;
   }
   C* acc = static_cast<C*>(mon.out) + loc;
 #pragma unroll
