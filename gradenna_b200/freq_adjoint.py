@@ -333,3 +333,16 @@ def freq_adjoint_objective(design_sigma, grid: Grid2D, objective, *, design_regi
     plan = _make_plan(grid, design_region, dft_freqs, env, source_ij, source_current, ports,
                       cpml, dtype, device, objective_monitors)
     return FreqAdjointObjective.apply(design_sigma, plan, objective)
+
+
+_3D_NAMES = ("FreqPhasors3D", "simulate_3d_freq", "port_dft_3d", "freq_adjoint_gradient_3d")
+
+
+def __getattr__(name):
+    # The reference keeps its 3D adjoint in this module (freq_adjoint.py:560-1065);
+    # here it lives in freq_adjoint3d and is re-exported lazily.
+    if name in _3D_NAMES:
+        from gradenna_b200 import freq_adjoint3d
+
+        return getattr(freq_adjoint3d, name)
+    raise AttributeError(f"module {__name__!r} has no attribute {name!r}")

@@ -1,0 +1,244 @@
+"""GPU checks of the 3D frequency-domain adjoint (gradenna_b200.freq_adjoint3d).
+
+The reference's acceptance cases (tests/test_freq_adjoint3d.py: 30^3 grid at
+3 mm, CPML 6, CW at 4 GHz with a 300-step ramp, 6000 steps, 6^3 design box)
+compare the two-run adjoint with jax.grad of the forward solve. jax is not
+available here, so the comparison is with central finite differences of the
+same discrete forward solve, which is the same quantity up to FD error. The
+tolerances are the reference's: cosine >= 0.9999 where the full gradient is
+formed, and a random-direction relative error <= 1e-2 (1.5e-2 for the
+single-point field objectives, 2e-2 for the two-tone case).
+
+Objectives: |Ez|^2 at a point (Jz path), the 6-face Poynting flux of a box
+(Mx/My/Mz path with Q_MAG), port |S11|^2 (port V/I rebuilt from the field
+phasors) and NTFF directivity (the six-component cotangents of ntff_3d).
+Region-limited DFT (objective_kind) must give the same gradient.
+"""
+
+import numpy as np
+import pytest
+import torch
+
+pytestmark = pytest.mark.gpu
+
+DX = 3e-3
+N = 30
+NPML = 6
+F0 = 4e9
+N_STEPS = 6000
+RAMP = 300
+DR = (slice(12, 18), slice(12, 18), slice(12, 18))
+DR_SHAPE = (6, 6, 6)
+CENTER = (15, 15, 15)
+FLUX_BOX = (9, 21, 9, 21, 9, 21)
+
+
+def _grid():
+    import gradenna_b200 as gb
+
+    return gb.Grid3D(N, N, N, DX, DX, DX)
+
+
+def _cw(grid, freqs=(F0,)):
+    n = np.arange(N_STEPS)
+    env = np.clip(n / float(RAMP), 0.0, 1.0)
+    cur = env * sum(np.sin(2.0 * np.pi * f * (n + 0.5) * grid.dt) for f in freqs)
+    return cur, env
+
+
+def _flux_box_3d(ph, grid, box):
+    """Outward Poynting flux through a 6-face box, face-patch averages as in
+    ntff_3d (the reference test's helper, restated in torch)."""
+    ex, ey, ez = ph.dft_ex, ph.dft_ey, ph.dft_ez
+    hx, hy, hz = ph.dft_hx, ph.dft_hy, ph.dft_hz
+    i0, i1, j0, j1, k0, k1 = box
+    dx, dy, dz = grid.dx, grid.dy, grid.dz
+    ic, jc, kc = slice(i0, i1), slice(j0, j1), slice(k0, k1)
+    icp, jcp, kcp = slice(i0 + 1, i1 + 1), slice(j0 + 1, j1 + 1), slice(k0 + 1, k1 + 1)
+
+    def re(a, b):
+        return torch.real(a * torch.conj(b))
+
+    p = 0.0
+    for i, s in ((i1, 1.0), (i0, -1.0)):
+        ey_f = 0.5 * (ey[:, i, jc, kc] + ey[:, i, jc, kcp])
+        ez_f = 0.5 * (ez[:, i, jc, kc] + ez[:, i, jcp, kc])
+        hy_f = 0.25 * (hy[:, i - 1, jc, kc] + hy[:, i, jc, kc] + hy[:, i - 1, jcp, kc] + hy[:, i, jcp, kc])
+        hz_f = 0.25 * (hz[:, i - 1, jc, kc] + hz[:, i, jc, kc] + hz[:, i - 1, jc, kcp] + hz[:, i, jc, kcp])
+        p = p + s * (0.5 * (re(ey_f, hz_f) - re(ez_f, hy_f))).sum((-1, -2)) * dy * dz
+    for j, s in ((j1, 1.0), (j0, -1.0)):
+        ex_f = 0.5 * (ex[:, ic, j, kc] + ex[:, ic, j, kcp])
+        ez_f = 0.5 * (ez[:, ic, j, kc] + ez[:, icp, j, kc])
+        hx_f = 0.25 * (hx[:, ic, j - 1, kc] + hx[:, ic, j, kc] + hx[:, icp, j - 1, kc] + hx[:, icp, j, kc])
+        hz_f = 0.25 * (hz[:, ic, j - 1, kc] + hz[:, ic, j, kc] + hz[:, ic, j - 1, kcp] + hz[:, ic, j, kcp])
+        p = p + s * (0.5 * (re(ez_f, hx_f) - re(ex_f, hz_f))).sum((-1, -2)) * dx * dz
+    for k, s in ((k1, 1.0), (k0, -1.0)):
+        ex_f = 0.5 * (ex[:, ic, jc, k] + ex[:, ic, jcp, k])
+        ey_f = 0.5 * (ey[:, ic, jc, k] + ey[:, icp, jc, k])
+        hx_f = 0.25 * (hx[:, ic, jc, k - 1] + hx[:, ic, jc, k] + hx[:, icp, jc, k - 1] + hx[:, icp, jc, k])
+        hy_f = 0.25 * (hy[:, ic, jc, k - 1] + hy[:, ic, jc, k] + hy[:, ic, jcp, k - 1] + hy[:, ic, jcp, k])
+        p = p + s * (0.5 * (re(ex_f, hy_f) - re(ey_f, hx_f))).sum((-1, -2)) * dx * dy
+    return p
+
+
+def _value(grid, obj, key, theta, common, port=None):
+    """Objective of one forward solve, with port phasors rebuilt from the
+    field phasors exactly as the adjoint path differentiates them."""
+    from gradenna_b200.freq_adjoint3d import _port_v_i_3d, simulate_3d_freq
+
+    ph = simulate_3d_freq(grid, **{f"design_{key}": theta}, **common)
+    if port is not None:
+        pv, pi = _port_v_i_3d(ph.dft_ez, ph.dft_hx, ph.dft_hy, grid, port, common["dft_freqs"])
+        ph = ph._replace(port_v=pv, port_i=pi)
+    return float(obj(ph))
+
+
+def _directional(grid, obj, key, theta, common, g, port=None, seed=0, rel_step=1e-3):
+    rng = np.random.default_rng(seed)
+    v = rng.normal(size=theta.shape)
+    v /= np.linalg.norm(v)
+    h = rel_step * float(np.abs(theta).max())
+    d_fd = (_value(grid, obj, key, theta + h * v, common, port)
+            - _value(grid, obj, key, theta - h * v, common, port)) / (2 * h)
+    d_adj = float(np.sum(np.asarray(g) * v))
+    return abs(d_adj - d_fd) / max(abs(d_fd), 1e-30), d_adj, d_fd
+
+
+def _adjoint(grid, obj, key, theta, env, common, **kw):
+    from gradenna_b200.freq_adjoint3d import freq_adjoint_gradient_3d
+
+    g = freq_adjoint_gradient_3d(grid, obj, **{f"design_{key}": theta}, env=env, **common, **kw)
+    g = g[key].cpu().numpy()
+    assert g.shape == DR_SHAPE and np.all(np.isfinite(g)) and np.abs(g).max() > 0
+    return g
+
+
+def _point_obj(ph):
+    e = ph.dft_ez[0, 19, 15, 15]
+    return e.real**2 + e.imag**2
+
+
+def test_field_sigma_full_gradient_matches_fd():
+    """|Ez|^2 at a point, sigma design: every design cell against central FD."""
+    import gradenna_b200 as gb
+
+    grid = _grid()
+    cur, env = _cw(grid)
+    common = dict(design_region=DR, dft_freqs=(F0,), source_ijk=(11, 15, 15),
+                  source_current=cur, cpml=gb.CPMLSpec(NPML))
+    sig0 = 0.02 * np.ones(DR_SHAPE)
+    g = _adjoint(grid, _point_obj, "sigma", sig0, env, common)
+    h = 2e-5
+    g_fd = np.zeros(DR_SHAPE)
+    for idx in np.ndindex(DR_SHAPE):
+        tp, tm = sig0.copy(), sig0.copy()
+        tp[idx] += h
+        tm[idx] -= h
+        g_fd[idx] = (_value(grid, _point_obj, "sigma", tp, common)
+                     - _value(grid, _point_obj, "sigma", tm, common)) / (2 * h)
+    cos = float(np.dot(g.ravel(), g_fd.ravel()) / (np.linalg.norm(g) * np.linalg.norm(g_fd)))
+    assert cos >= 0.9999, f"field/sigma cosine {cos:.6f}"
+    v = np.random.default_rng(0).normal(size=DR_SHAPE)
+    rel = abs(np.sum(g * v) - np.sum(g_fd * v)) / abs(np.sum(g_fd * v))
+    assert rel <= 1.5e-2, f"field/sigma directional rel. error {rel:.2e}"
+
+
+def test_field_eps_r_matches_fd():
+    import gradenna_b200 as gb
+
+    grid = _grid()
+    cur, env = _cw(grid)
+    common = dict(design_region=DR, dft_freqs=(F0,), source_ijk=(11, 15, 15),
+                  source_current=cur, cpml=gb.CPMLSpec(NPML))
+    eps0 = 2.0 * np.ones(DR_SHAPE)
+    g = _adjoint(grid, _point_obj, "eps_r", eps0, env, common)
+    rel, a, b = _directional(grid, _point_obj, "eps_r", eps0, common, g)
+    assert rel <= 1.5e-2, f"field/eps_r directional rel. error {rel:.2e} ({a} vs {b})"
+
+
+def test_flux_sigma_and_two_tones_match_fd():
+    """Flux objective (H cotangents -> Mx/My/Mz with Q_MAG), one and two tones."""
+    import gradenna_b200 as gb
+
+    grid = _grid()
+    sig0 = 0.02 * np.ones(DR_SHAPE)
+    for freqs, tol in (((F0,), 1e-2), ((3.4e9, 4.6e9), 2e-2)):
+        cur, env = _cw(grid, freqs)
+
+        def obj(ph):
+            return _flux_box_3d(ph, grid, FLUX_BOX).sum()
+
+        common = dict(design_region=DR, dft_freqs=freqs, source_ijk=CENTER, source_current=cur,
+                      cpml=gb.CPMLSpec(NPML))
+        g = _adjoint(grid, obj, "sigma", sig0, env, common)
+        rel, a, b = _directional(grid, obj, "sigma", sig0, common, g)
+        assert rel <= tol, f"flux {len(freqs)}-tone directional rel. error {rel:.2e} ({a} vs {b})"
+
+
+def test_s11_sigma_matches_fd_and_port_regions():
+    import gradenna_b200 as gb
+    from gradenna_b200.sparams import s11_power_wave
+
+    grid = _grid()
+    cur, env = _cw(grid)
+    rs = 50.0
+
+    def obj(ph):
+        s = s11_power_wave(ph.port_v[0, 0], ph.port_i[0, 0], rs)
+        return s.real**2 + s.imag**2
+
+    common = dict(design_region=DR, dft_freqs=(F0,), port_ijk=CENTER, port_voltage=cur,
+                  port_resistance=rs, cpml=gb.CPMLSpec(NPML))
+    sig0 = 0.05 * np.ones(DR_SHAPE)
+    g = _adjoint(grid, obj, "sigma", sig0, env, common)
+    rel, a, b = _directional(grid, obj, "sigma", sig0, common, g, port=CENTER)
+    assert rel <= 1e-2, f"S11/sigma directional rel. error {rel:.2e} ({a} vs {b})"
+    g_reg = _adjoint(grid, obj, "sigma", sig0, env, common, objective_kind="port")
+    assert np.allclose(g_reg, g, rtol=1e-9, atol=1e-12 * np.abs(g).max())
+
+
+def test_ntff_directivity_matches_fd_and_box_regions():
+    """loss = -D(theta0, phi0) through ntff_3d and directivity_3d."""
+    import gradenna_b200 as gb
+    from gradenna_b200.fdtd3d import DFTMonitor
+    from gradenna_b200.ntff import directivity_3d, ntff_3d
+
+    grid = _grid()
+    cur, env = _cw(grid)
+    thetas = np.linspace(0.05, np.pi - 0.05, 9)
+    phis = np.linspace(0.0, 2 * np.pi, 12, endpoint=False)
+
+    def obj(ph):
+        mon = DFTMonitor(torch.tensor([F0]), ph.dft_ex, ph.dft_ey, ph.dft_ez, ph.dft_hx,
+                         ph.dft_hy, ph.dft_hz)
+        ef = ntff_3d(mon, grid, NPML + 1, (F0,), thetas, phis)
+        d = directivity_3d(ef[..., 0], ef[..., 1], thetas, phis)
+        return -d[0, 4, 0]
+
+    common = dict(design_region=DR, dft_freqs=(F0,), source_ijk=CENTER, source_current=cur,
+                  cpml=gb.CPMLSpec(NPML))
+    sig0 = 0.02 * np.ones(DR_SHAPE)
+    g = _adjoint(grid, obj, "sigma", sig0, env, common)
+    rel, a, b = _directional(grid, obj, "sigma", sig0, common, g)
+    assert rel <= 1e-2, f"NTFF directivity directional rel. error {rel:.2e} ({a} vs {b})"
+    g_reg = _adjoint(grid, obj, "sigma", sig0, env, common, objective_kind="ntff_box",
+                     box_margin=NPML + 1)
+    assert np.allclose(g_reg, g, rtol=1e-9, atol=1e-12 * np.abs(g).max())
+
+
+def test_bad_arguments():
+    import gradenna_b200 as gb
+    from gradenna_b200.freq_adjoint3d import freq_adjoint_gradient_3d
+
+    grid = _grid()
+    cur, env = _cw(grid)
+    common = dict(design_region=DR, dft_freqs=(F0,), source_ijk=CENTER, source_current=cur,
+                  cpml=gb.CPMLSpec(NPML), env=env)
+    with pytest.raises(ValueError):
+        freq_adjoint_gradient_3d(grid, _point_obj, **common)
+    with pytest.raises(ValueError):
+        freq_adjoint_gradient_3d(grid, _point_obj, design_sigma=np.zeros(DR_SHAPE),
+                                 objective_kind="ntff_box", **common)
+    with pytest.raises(ValueError):
+        freq_adjoint_gradient_3d(grid, _point_obj, design_sigma=np.zeros(DR_SHAPE),
+                                 backend="jax", **common)
