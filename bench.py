@@ -68,6 +68,23 @@ RAMP = 300
 RS = 50.0
 
 
+# 3D patch workload (Yee, float32): 160 x 160 x 64 at 0.5 mm, CPML 10,
+# 6000 steps, PEC-like ground sheet under a 4-cell eps_r = 4.4 substrate,
+# 96 x 96 single-plane copper design sheet, vertical 50-ohm port, 11
+# frequencies over 2-3 GHz.
+P3_SHAPE = (160, 160, 64)
+P3_D = 0.5e-3
+P3_NPML = 10
+P3_STEPS = 6000
+P3_FREQS = tuple(np.linspace(2.0e9, 3.0e9, 11))
+P3_NDES = 96
+P3_SIG_FIXED = 1.0e7
+P3_T_CU = 35e-6
+P3_BOX = P3_NPML + 2
+P3_THETAS = tuple(np.linspace(0.0, np.pi, 13))
+P3_PHIS = tuple(np.linspace(0.0, 2 * np.pi, 16, endpoint=False))
+
+
 def parse():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -76,8 +93,13 @@ def parse():
     ap.add_argument("--impl", choices=("ours", "reference"), default="ours")
     ap.add_argument("--dtype", choices=("f32", "f64"), default="f32")
     ap.add_argument("--grid", type=int, default=N_GRID)
-    ap.add_argument("--time-steps", type=int, default=N_STEPS)
-    return ap.parse_args()
+    ap.add_argument("--time-steps", type=int, default=None,
+                    help="time steps per run (default: 8000 for tm2d, 6000 for patch3d)")
+    ap.add_argument("--workload", choices=("tm2d", "patch3d"), default="tm2d")
+    args = ap.parse_args()
+    if args.time_steps is None:
+        args.time_steps = N_STEPS if args.workload == "tm2d" else P3_STEPS
+    return args
 
 
 def workload(seed: int, n_grid: int, n_steps: int):
@@ -101,6 +123,72 @@ def workload(seed: int, n_grid: int, n_steps: int):
     ports = tuple((int(i * s), int(j * s)) for i, j in PORTS)
     box = tuple(int(v * s) for v in BOX)
     return dict(grid=grid, design=design, sigma_d=sigma_d, env=env, vs=vs, ports=ports, box=box)
+
+
+def workload3d(seed: int, n_steps: int):
+    """Host inputs of the 3D patch workload for design `seed`."""
+    import torch
+
+    from gradenna_b200.grid import Grid3D
+    from gradenna_b200.materials import sheet_conductivity, sigma_from_density
+    from gradenna_b200.topopt import seeded_density
+
+    nx, ny, nz = P3_SHAPE
+    grid = Grid3D(nx, ny, nz, P3_D, P3_D, P3_D)
+    kg = P3_NPML + 3          # ground sheet layer
+    kp = kg + 4 + 1           # design (patch) layer above a 4-cell substrate
+    d0 = (nx - P3_NDES) // 2
+    d1 = d0 + P3_NDES
+    g0, g1 = d0 - 6, d1 + 6
+    eps_r = np.ones(P3_SHAPE)
+    sigma = np.zeros(P3_SHAPE)
+    eps_r[g0:g1, g0:g1, kg + 1:kp] = 4.4
+    sigma[g0:g1, g0:g1, kg] = P3_SIG_FIXED
+    pi, pj = (d0 + d1) // 2, d0 + P3_NDES // 4
+    sigma[pi, pj, kg + 1:kp - 1] = P3_SIG_FIXED  # feed pin up to the port gap
+    rho = seeded_density((P3_NDES, P3_NDES), seed=seed, radius_cells=3.0, beta=8.0, eta=0.5,
+                         device="cpu", dtype=torch.float64).numpy()
+    rho[pi - d0, pj - d0] = 1.0  # feed pad is metal
+    sig_d = (sheet_conductivity(1.0, P3_T_CU, P3_D)
+             * np.asarray(sigma_from_density(rho), np.float64))[:, :, None]
+    n = np.arange(n_steps)
+    env = np.clip(n / float(RAMP), 0.0, 1.0)
+    vs = env * sum(np.sin(2 * np.pi * f * (n + 0.5) * grid.dt) for f in P3_FREQS)
+    design = (slice(d0, d1), slice(d0, d1), slice(kp, kp + 1))
+    return dict(grid=grid, design=design, sigma_d=sig_d, env=env, vs=vs, port=(pi, pj, kp - 1),
+                eps_bg=eps_r, sig_bg=sigma)
+
+
+def make_objective3d(grid):
+    """sum_k |S11_k|^2 - mean_k D_k(theta = 0) from the NTFF of the box."""
+    import torch
+
+    from gradenna_b200.fdtd3d import DFTMonitor
+    from gradenna_b200.ntff import directivity_3d, ntff_3d
+    from gradenna_b200.sparams import s11_power_wave
+
+    def obj(ph):
+        s = s11_power_wave(ph.port_v[:, 0], ph.port_i[:, 0], RS)
+        mon = DFTMonitor(torch.tensor(P3_FREQS), ph.dft_ex, ph.dft_ey, ph.dft_ez, ph.dft_hx,
+                         ph.dft_hy, ph.dft_hz)
+        ef = ntff_3d(mon, grid, P3_BOX, P3_FREQS, P3_THETAS, P3_PHIS)
+        d = directivity_3d(ef[..., 0], ef[..., 1], P3_THETAS, P3_PHIS)
+        return (s.real**2 + s.imag**2).sum() - d[:, 0, 0].mean()
+
+    return obj
+
+
+def gradient_call3d(w, sigma_dev, vs_dev, dtype):
+    import gradenna_b200 as gb
+    from gradenna_b200.freq_adjoint3d import freq_adjoint_gradient_3d
+
+    grid = w["grid"]
+    return freq_adjoint_gradient_3d(
+        grid, make_objective3d(grid), design_sigma=sigma_dev, design_region=w["design"],
+        dft_freqs=P3_FREQS, env=w["env"], port_ijk=w["port"], port_voltage=vs_dev,
+        port_resistance=RS, cpml=gb.CPMLSpec(P3_NPML), dtype=dtype,
+        objective_kind=("port", "ntff_box"), box_margin=P3_BOX,
+        eps_r_background=w["eps_bg"], sigma_background=w["sig_bg"])["sigma"]
 
 
 def make_objective(grid, box):
@@ -237,9 +325,10 @@ def measured_peak():
         return 6650.0, "fallback"
 
 
-def profiled_traffic():
-    """dram bytes per tm_tb 4-step block from the committed ncu summary, or None."""
-    path = os.path.join(ROOT, "profiles", "tm_tb_1024.txt")
+def profiled_traffic(name):
+    """DRAM bytes per block of the dominant kernel from a committed ncu summary
+    (its traffic_bytes_per_launch line), or None."""
+    path = os.path.join(ROOT, "profiles", name)
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_launch:"):
@@ -277,26 +366,27 @@ def run_reference(args):
     world, rank, _ = dist_setup(args)
     if rank != 0:
         return 0
-    w = workload(0, args.grid, args.time_steps)
+    case = make_case(args, 0)
+    w = case["w"]
     dt_np = np.float32 if args.dtype == "f32" else np.float64
     vals = []
     n_s = None
     for k in range(args.warmup + args.steps):
-        v, n_s, _ = cpu_sample(w, dt_np, target_s=6.0)
+        v, n_s, t_s = case["cpu"](dt_np)
         if k >= args.warmup:
             vals.append(v)
     value = float(np.mean(vals))
-    cores = os.cpu_count()
+    cores = os.cpu_count() if args.workload == "tm2d" else 1
     line = {
         "impl": "reference", "metric": "Gcell-steps/s fwd+adjoint", "value": value,
         "unit": "Gcell-steps/s", "n_gpus": args.gpus, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": 2 * w["grid"].nx * w["grid"].ny * args.time_steps / value / 1e6,
+        "warmup": args.warmup,
+        "ms_per_step": 2 * case["cells"] * args.time_steps / value / 1e6,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": args.dtype,
         "data": "synthetic",
-        "config": config_dict(args, w),
+        "config": case["config"],
         "cpu_baseline": {"value": value, "unit": "Gcell-steps/s", "cores": cores, "kind": "port",
-                         "sample": f"forward + adjoint-shaped runs of {n_s} of {args.time_steps} "
-                                   f"steps on the full {args.grid}^2 grid per step"},
+                         "sample": case["cpu_what"](n_s, t_s) + " per step"},
         "e2e": {"value": value, "unit": "Gcell-steps/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -311,6 +401,72 @@ def config_dict(args, w):
                     f"K={len(FREQS)} DFT (complex128), P_rad - |S11|^2 objective, freq-adjoint "
                     f"gradient over a {w['sigma_d'].shape[0]}x{w['sigma_d'].shape[1]} design",
         "grid": [g.nx, g.ny], "time_steps": args.time_steps, "n_freq": len(FREQS),
+        "design_cells": int(w["sigma_d"].size), "parallelism": f"replicas x{args.gpus}",
+        "l2": "flushed (256 MiB write) before every timed step",
+    }
+
+
+def cpu_sample3d(w, dtype_np, target_s: float = 10.0):
+    """Time n_s steps of the numpy 3D oracle on the full patch grid (one
+    forward run: ground, substrate, design sheet, port); n_s is sized so the
+    sample takes about target_s."""
+    from oracle import fdtd2d_np as onp
+    from oracle import fdtd3d_np as o3
+
+    g = w["grid"]
+    og = o3.Grid3D(g.nx, g.ny, g.nz, g.dx, g.dy, g.dz)
+    sigma = w["sig_bg"].copy()
+    sigma[w["design"]] = w["sigma_d"]
+
+    def run(n_s):
+        t0 = time.perf_counter()
+        o3.simulate_3d(og, eps_r=w["eps_bg"], sigma=sigma, port_ijk=w["port"],
+                       port_voltage=w["vs"][:n_s], port_resistance=RS,
+                       cpml=onp.CPMLSpec(P3_NPML), dtype=dtype_np)
+        return time.perf_counter() - t0
+
+    probe = 2
+    t = run(probe)
+    n_s = int(np.clip(target_s / max(t, 1e-6) * probe, 2, len(w["vs"])))
+    t = run(n_s)
+    return g.nx * g.ny * g.nz * n_s / t / 1e9, n_s, t
+
+
+def make_case(args, seed):
+    """The workload's inputs and per-workload figures for the JSON line."""
+    if args.workload == "tm2d":
+        w = workload(seed, args.grid, args.time_steps)
+        mons = monitors_for(w)
+        g = w["grid"]
+        return dict(
+            w=w, call=lambda s_, v_, fdt: gradient_call(w, s_, v_, fdt, mons),
+            cells=g.nx * g.ny, tb=4, words=8, config=config_dict(args, w),
+            kernel="tm_tb 4-step block over the grid (time loop incl. DFT folds)",
+            traffic=profiled_traffic("tm_tb_1024.txt"),
+            cpu=lambda dt: cpu_sample(w, dt),
+            cpu_what=lambda n_s, t: (f"C oracle, forward + adjoint-shaped runs of {n_s} steps on "
+                                     f"the full {g.nx}^2 grid ({t:.1f} s)"))
+    w = workload3d(seed, args.time_steps)
+    g = w["grid"]
+    return dict(
+        w=w, call=lambda s_, v_, fdt: gradient_call3d(w, s_, v_, fdt),
+        cells=g.nx * g.ny * g.nz, tb=1, words=14, config=config3d(args, w),
+        kernel="yee_h + yee_e, one time step over the volume (time loop incl. DFT folds)",
+        traffic=profiled_traffic("yee_patch3d.txt"),
+        cpu=lambda dt: cpu_sample3d(w, dt),
+        cpu_what=lambda n_s, t: (f"numpy 3D oracle, one forward run of {n_s} steps on the full "
+                                 f"{g.nx}x{g.ny}x{g.nz} grid ({t:.1f} s)"))
+
+
+def config3d(args, w):
+    g = w["grid"]
+    return {
+        "workload": f"3D Yee patch {g.nx}x{g.ny}x{g.nz} @0.5mm, CPML {P3_NPML}, "
+                    f"{args.time_steps} steps, ground sheet + 4-cell eps_r 4.4 substrate, "
+                    f"{P3_NDES}x{P3_NDES} design sheet, 50-ohm port, K={len(P3_FREQS)} DFT "
+                    f"(complex128, port + NTFF faces + design), objective sum|S11|^2 - mean "
+                    f"D(theta=0), freq-adjoint gradient",
+        "grid": [g.nx, g.ny, g.nz], "time_steps": args.time_steps, "n_freq": len(P3_FREQS),
         "design_cells": int(w["sigma_d"].size), "parallelism": f"replicas x{args.gpus}",
         "l2": "flushed (256 MiB write) before every timed step",
     }
@@ -335,14 +491,14 @@ def run_ours(args):
     from gradenna_b200 import _native
 
     fdt = torch.float32 if args.dtype == "f32" else torch.float64
-    w = workload(rank, args.grid, args.time_steps)
-    mons = monitors_for(w)
+    case = make_case(args, rank)
+    w = case["w"]
     sigma_dev = torch.as_tensor(w["sigma_d"], device=dev)
     vs_dev = torch.as_tensor(w["vs"], device=dev)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
 
     for _ in range(args.warmup):
-        gradient_call(w, sigma_dev, vs_dev, fdt, mons)
+        case["call"](sigma_dev, vs_dev, fdt)
     torch.cuda.synchronize()
 
     def barrier():
@@ -359,7 +515,7 @@ def run_ours(args):
             flush.fill_(1.0)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
             e0.record()
-            g = gradient_call(w, sigma_dev, vs_dev, fdt, mons)
+            g = case["call"](sigma_dev, vs_dev, fdt)
             e1.record()
             torch.cuda.synchronize()
             times.append(e0.elapsed_time(e1) / 1e3)
@@ -382,7 +538,7 @@ def run_ours(args):
         e0.record()
         sd = sig_h.to(dev, non_blocking=True)
         vd = vs_h.to(dev, non_blocking=True)
-        gg = gradient_call(w, sd, vd, fdt, mons)
+        gg = case["call"](sd, vd, fdt)
         out_h.copy_(gg, non_blocking=True)
         e1.record()
         torch.cuda.synchronize()
@@ -393,14 +549,13 @@ def run_ours(args):
 
     t_step, t_e2e = max_over_ranks(pg, [t_step, t_e2e], dev)
 
-    g_ = w["grid"]
-    cell_steps = 2 * g_.nx * g_.ny * args.time_steps
+    cell_steps = 2 * case["cells"] * args.time_steps
     value = world * cell_steps / t_step / 1e9
     e2e = world * cell_steps / t_e2e / 1e9
     esize = 4 if fdt == torch.float32 else 8
-    tb = 4
-    # 8 words per cell-step (Ez/Hx/Hy read + written, ca/cb read) over TB steps.
-    algo_bytes = tb * 8 * esize * g_.nx * g_.ny
+    # Words per cell-step: 2D 8 (Ez/Hx/Hy read + written, ca/cb read), 3D 14
+    # (six fields read + written, ca/cb read); one block = tb time steps.
+    algo_bytes = case["tb"] * case["words"] * esize * case["cells"]
     achieved = algo_bytes / t_block / 1e9
     peak, peak_kind = measured_peak()
     h2d = w["sigma_d"].nbytes + w["vs"].nbytes
@@ -408,20 +563,20 @@ def run_ours(args):
 
     cpu = None
     if rank == 0:
-        v_cpu, n_s, t_cpu = cpu_sample(w, np.float32 if fdt == torch.float32 else np.float64)
-        cpu = {"value": v_cpu, "unit": "Gcell-steps/s", "cores": os.cpu_count(), "kind": "port",
-               "sample": f"C oracle, forward + adjoint-shaped runs of {n_s} steps on the full "
-                         f"{g_.nx}^2 grid ({t_cpu:.1f} s)"}
+        v_cpu, n_s, t_cpu = case["cpu"](np.float32 if fdt == torch.float32 else np.float64)
+        cpu = {"value": v_cpu, "unit": "Gcell-steps/s",
+               "cores": os.cpu_count() if args.workload == "tm2d" else 1, "kind": "port",
+               "sample": case["cpu_what"](n_s, t_cpu)}
     if rank == 0:
         line = {
             "metric": "Gcell-steps/s fwd+adjoint", "value": value, "unit": "Gcell-steps/s",
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": args.dtype, "data": "synthetic",
-            "config": config_dict(args, w),
+            "config": case["config"],
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": profiled_traffic(),
-                         "kernel": "tm_tb 4-step block over the grid (time loop incl. DFT folds)", "peak_source": peak_kind,
+                         "frac": achieved / peak, "traffic": case["traffic"],
+                         "kernel": case["kernel"], "peak_source": peak_kind,
                          "algorithmic_bytes_per_launch": algo_bytes,
                          "launch_us": t_block * 1e6,
                          "loop_share_of_step": loop_ms / 1e3 / (t_step * args.steps)},

@@ -1,6 +1,7 @@
 // Error reporting, version string and the per-device capture stream.
 #include <atomic>
 #include <mutex>
+#include <vector>
 
 #include "common.cuh"
 
@@ -22,6 +23,72 @@ const char* last_error() { return g_last_error.c_str(); }
 static std::atomic<uint64_t> g_launches{0};
 void count_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 uint64_t total_launches() { return g_launches.load(std::memory_order_relaxed); }
+
+struct LoopRecord {
+  cudaEvent_t a, b;
+  double cell_steps;
+  int64_t blocks;
+};
+static std::mutex g_loop_mu;
+static std::vector<LoopRecord> g_loops;
+constexpr size_t kMaxLoopRecords = 4096;
+
+LoopTimer::LoopTimer(cudaStream_t s, double cell_steps, int64_t blocks)
+    : s_(s), cells_(cell_steps), blocks_(blocks) {
+  {
+    std::lock_guard<std::mutex> lk(g_loop_mu);
+    if (g_loops.size() >= kMaxLoopRecords) return;
+  }
+  if (cudaEventCreate(&a_) != cudaSuccess || cudaEventCreate(&b_) != cudaSuccess ||
+      cudaEventRecord(a_, s_) != cudaSuccess) {
+    release();
+    cudaGetLastError();
+  }
+}
+
+void LoopTimer::release() {
+  if (a_) cudaEventDestroy(a_);
+  if (b_) cudaEventDestroy(b_);
+  a_ = b_ = nullptr;
+}
+
+void LoopTimer::stop(bool ok) {
+  if (!a_ || !b_) return;
+  if (!ok || cudaEventRecord(b_, s_) != cudaSuccess) {
+    release();
+    return;
+  }
+  std::lock_guard<std::mutex> lk(g_loop_mu);
+  g_loops.push_back({a_, b_, cells_, blocks_});
+  a_ = b_ = nullptr;
+}
+
+LoopTimer::~LoopTimer() { release(); }
+
+static int loop_stats(double* loop_ms, double* cell_steps, int64_t* blocks, int32_t reset) {
+  std::lock_guard<std::mutex> lk(g_loop_mu);
+  double ms = 0.0, cs = 0.0;
+  int64_t nb = 0;
+  for (auto& r : g_loops) {
+    GDN_TRY_CUDA(cudaEventSynchronize(r.b));
+    float t = 0.f;
+    GDN_TRY_CUDA(cudaEventElapsedTime(&t, r.a, r.b));
+    ms += t;
+    cs += r.cell_steps;
+    nb += r.blocks;
+  }
+  if (loop_ms) *loop_ms = ms;
+  if (cell_steps) *cell_steps = cs;
+  if (blocks) *blocks = nb;
+  if (reset) {
+    for (auto& r : g_loops) {
+      cudaEventDestroy(r.a);
+      cudaEventDestroy(r.b);
+    }
+    g_loops.clear();
+  }
+  return GDN_OK;
+}
 
 cudaStream_t capture_stream() {
   static std::mutex mu;
@@ -52,3 +119,8 @@ extern "C" const char* gdn_version(void) { return "gradenna_b200 0.1 (sm_100a)";
 extern "C" const char* gdn_last_error(void) { return gdn::last_error(); }
 
 extern "C" uint64_t gdn_kernel_launches(void) { return gdn::total_launches(); }
+
+extern "C" int gdn_tm_loop_stats(double* loop_ms, double* cell_steps, int64_t* blocks,
+                                 int32_t reset) {
+  return gdn::loop_stats(loop_ms, cell_steps, blocks, reset);
+}

@@ -56,6 +56,24 @@ struct Carve {
 void count_launches(uint64_t n);
 uint64_t total_launches();
 
+// Device time of one run's time loop for gdn_tm_loop_stats: CUDA events
+// recorded on the caller's stream before and after the loop, resolved
+// lazily by the stats call. `blocks` counts launches of the dominant kernel
+// over the whole grid (TB-step blocks in 2D, time steps in 3D).
+class LoopTimer {
+ public:
+  LoopTimer(cudaStream_t s, double cell_steps, int64_t blocks);
+  void stop(bool ok);
+  ~LoopTimer();
+
+ private:
+  void release();
+  cudaEvent_t a_ = nullptr, b_ = nullptr;
+  cudaStream_t s_;
+  double cells_;
+  int64_t blocks_;
+};
+
 // A private non-blocking stream per device used only to capture graphs; the
 // captured graphs are launched on the caller's stream.
 cudaStream_t capture_stream();

@@ -1321,51 +1321,6 @@ static int finalize(const GdnTmParams* p, const GdnTmBuffers* b, const Run<T>& R
   return GDN_OK;
 }
 
-// Time-loop timing for gdn_tm_loop_stats: events recorded on the caller's
-// stream around the replay of the time loop of every run, resolved lazily.
-struct LoopRecord {
-  cudaEvent_t a, b;
-  double cell_steps;
-  int64_t blocks;
-};
-static std::mutex g_loop_mu;
-static std::vector<LoopRecord> g_loops;
-constexpr size_t kMaxLoopRecords = 4096;
-
-struct LoopTimer {
-  cudaEvent_t a = nullptr, b = nullptr;
-  cudaStream_t s;
-  double cells;
-  int64_t blocks;
-  LoopTimer(cudaStream_t s_, double c, int64_t n) : s(s_), cells(c), blocks(n) {
-    {
-      std::lock_guard<std::mutex> lk(g_loop_mu);
-      if (g_loops.size() >= kMaxLoopRecords) return;
-    }
-    if (cudaEventCreate(&a) != cudaSuccess || cudaEventCreate(&b) != cudaSuccess ||
-        cudaEventRecord(a, s) != cudaSuccess) {
-      release();
-      cudaGetLastError();
-    }
-  }
-  void release() {
-    if (a) cudaEventDestroy(a);
-    if (b) cudaEventDestroy(b);
-    a = b = nullptr;
-  }
-  void stop(bool ok) {
-    if (!a || !b) return;
-    if (!ok || cudaEventRecord(b, s) != cudaSuccess) {
-      release();
-      return;
-    }
-    std::lock_guard<std::mutex> lk(g_loop_mu);
-    g_loops.push_back({a, b, cells, blocks});
-    a = b = nullptr;
-  }
-  ~LoopTimer() { release(); }
-};
-
 template <typename T>
 static int run(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuffers* b,
                cudaStream_t stream) {
@@ -1459,32 +1414,6 @@ static int run(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuffers*
 
 }  // namespace tm2d
 }  // namespace gdn
-
-extern "C" int gdn_tm_loop_stats(double* loop_ms, double* cell_steps, int64_t* blocks,
-                                 int32_t reset) {
-  std::lock_guard<std::mutex> lk(gdn::tm2d::g_loop_mu);
-  double ms = 0.0, cs = 0.0;
-  int64_t nb = 0;
-  for (auto& r : gdn::tm2d::g_loops) {
-    GDN_TRY_CUDA(cudaEventSynchronize(r.b));
-    float t = 0.f;
-    GDN_TRY_CUDA(cudaEventElapsedTime(&t, r.a, r.b));
-    ms += t;
-    cs += r.cell_steps;
-    nb += r.blocks;
-  }
-  if (loop_ms) *loop_ms = ms;
-  if (cell_steps) *cell_steps = cs;
-  if (blocks) *blocks = nb;
-  if (reset) {
-    for (auto& r : gdn::tm2d::g_loops) {
-      cudaEventDestroy(r.a);
-      cudaEventDestroy(r.b);
-    }
-    gdn::tm2d::g_loops.clear();
-  }
-  return GDN_OK;
-}
 
 extern "C" int gdn_tm_workspace_size(const GdnTmParams* p, const GdnTmPoints* pts, int f64,
                                      size_t* bytes) {

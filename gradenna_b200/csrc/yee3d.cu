@@ -19,6 +19,7 @@
 // sum_t ph[t,k] x_t to the accumulators. One chunk of R steps is captured as
 // a CUDA graph and replayed; kernels read the absolute step from a counter.
 #include <algorithm>
+#include <array>
 #include <cmath>
 
 #include "common.cuh"
@@ -34,6 +35,16 @@ constexpr int NC = 6;  // components: ex ey ez hx hy hz
 struct Pt3 {
   int m, i, j, k;
 };
+
+// One monitor's part inside one CTA box (a single i-plane): cells j in
+// [j0, j1), k in [k0, k1) of component comp go to ring index
+// base + (i * s1 + j) * s2 + k. Binned per CTA on the host.
+struct MonW3 {
+  int j0, j1, k0, k1, comp, s2;
+  long long base;
+  int s1, pad;
+};
+constexpr int MAXF = 64;  // monitors whose offsets the fold stages in shared memory
 
 struct Mon3 {
   int comp, lo0, lo1, lo2, s0, s1, s2, pad;
@@ -69,6 +80,8 @@ struct Dev3 {
   long long mon_cells;
   int n_mons;
   const Mon3* mons;
+  const int* mw_off;  // per-CTA CSR over mw
+  const MonW3* mw;
   const int* step_base;
 };
 
@@ -117,18 +130,18 @@ __device__ __forceinline__ T cpml(const Dev3<T>& d, int ax, int s, int n_samples
   return diff;
 }
 
-// Monitored cells of this CTA's box for components in [c0, c1).
+// Monitored cells of this CTA's box for components in [c0, c1): only the
+// monitor parts binned to this CTA.
 template <typename T>
-__device__ __forceinline__ void write_monitors(const Dev3<T>& d, int c0, int c1, int n, int i,
-                                               int j, int k) {
-  if (d.n_mons == 0) return;
+__device__ __forceinline__ void write_monitors(const Dev3<T>& d, int c0, int c1, int n, int cta,
+                                               int i, int j, int k) {
+  const int qb = d.mw_off[cta], qe = d.mw_off[cta + 1];
+  if (qb == qe) return;
   T* slot = d.mring + (long long)(n % d.R) * d.mon_cells;
-  for (int mm = 0; mm < d.n_mons; ++mm) {
-    const Mon3 mo = d.mons[mm];
-    if (mo.comp < c0 || mo.comp >= c1) continue;
-    const int a = i - mo.lo0, b = j - mo.lo1, c = k - mo.lo2;
-    if (a < 0 || a >= mo.s0 || b < 0 || b >= mo.s1 || c < 0 || c >= mo.s2) continue;
-    slot[mo.off + ((long long)a * mo.s1 + b) * mo.s2 + c] = d.f[mo.comp][at(d, i, j, k)];
+  for (int q = qb; q < qe; ++q) {
+    const MonW3 w = d.mw[q];
+    if (w.comp < c0 || w.comp >= c1 || j < w.j0 || j >= w.j1 || k < w.k0 || k >= w.k1) continue;
+    slot[w.base + ((long long)i * w.s1 + j) * w.s2 + k] = d.f[w.comp][at(d, i, j, k)];
   }
 }
 
@@ -189,7 +202,7 @@ __global__ void __launch_bounds__(NT) yee_h(Dev3<T> d, int sub) {
   }
   if (d.n_mons > 0) {
     __syncthreads();
-    if (j < ny && k < nz) write_monitors(d, 3, 6, n, i, j, k);
+    if (j < ny && k < nz) write_monitors(d, 3, 6, n, cta, i, j, k);
   }
 }
 
@@ -274,7 +287,7 @@ __global__ void __launch_bounds__(NT) yee_e(Dev3<T> d, int sub) {
   }
   if (d.n_mons > 0) {
     __syncthreads();
-    if (j < ny && k < nz) write_monitors(d, 0, 3, n, i, j, k);
+    if (j < ny && k < nz) write_monitors(d, 0, 3, n, cta, i, j, k);
   }
 }
 
@@ -296,25 +309,56 @@ __global__ void __launch_bounds__(256) yee_fold(Dev3<T> d, int cnt) {
     sph[2 * (cnt * K + idx) + 1] = A(ph.y);
   }
   __syncthreads();
-  const Mon3 mon = d.mons[blockIdx.y];
+  __shared__ long long sOff[MAXF];
+  const int nm = d.n_mons;
+  if (nm <= MAXF)
+    for (int m = threadIdx.x; m < nm; m += blockDim.x) sOff[m] = d.mons[m].off;
+  __syncthreads();
   const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (r >= mon.count) return;
+  if (r >= d.mon_cells) return;
+  int lo = 0, hi = nm - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    const long long o = nm <= MAXF ? sOff[mid] : d.mons[mid].off;
+    if (o <= r)
+      lo = mid;
+    else
+      hi = mid - 1;
+  }
+  const Mon3 mon = d.mons[lo];
+  const long long loc = r - mon.off;
   const A* ph = sph + (mon.comp < 3 ? 0 : 2 * cnt * K);
   A are[KM], aim[KM];
 #pragma unroll
   for (int kk = 0; kk < KM; ++kk) are[kk] = aim[kk] = A(0);
-  const T* base = d.mring + mon.off + r;
-#pragma unroll 4
-  for (int t = 0; t < cnt; ++t) {
-    const A x = A(base[(long long)((n0 + t) % d.R) * d.mon_cells]);
+  const T* base = d.mring + r;
+  int slot = n0 % d.R;
+  for (int t0 = 0; t0 < cnt; t0 += 8) {
+    A x[8];
 #pragma unroll
-    for (int kk = 0; kk < KM; ++kk)
-      if (kk < K) {
-        are[kk] += ph[2 * (t * K + kk)] * x;
-        aim[kk] += ph[2 * (t * K + kk) + 1] * x;
+    for (int u = 0; u < 8; ++u) {
+      x[u] = A(0);
+      if (t0 + u < cnt) {
+        const int sl = slot + u >= d.R ? slot + u - d.R : slot + u;
+        x[u] = A(base[(long long)sl * d.mon_cells]);
       }
+    }
+#pragma unroll
+    for (int u = 0; u < 8; ++u) {
+      if (t0 + u < cnt) {
+        const A* pt = ph + 2 * (t0 + u) * K;
+#pragma unroll
+        for (int kk = 0; kk < KM; ++kk)
+          if (kk < K) {
+            are[kk] += pt[2 * kk] * x[u];
+            aim[kk] += pt[2 * kk + 1] * x[u];
+          }
+      }
+    }
+    slot += 8;
+    if (slot >= d.R) slot -= d.R;
   }
-  C* acc = static_cast<C*>(mon.out) + r;
+  C* acc = static_cast<C*>(mon.out) + loc;
 #pragma unroll
   for (int kk = 0; kk < KM; ++kk)
     if (kk < K) {
@@ -421,9 +465,41 @@ static void comp_shape(int c, int nx, int ny, int nz, int s[3]) {
 
 struct Layout3 {
   int sy = 0, sz = 0, gj = 0, gk = 0, n_cta = 0, R = 32;
-  long long vol = 0, mon_cells = 0;
-  size_t fields, psi, zero_end, off[7], pts[7], mons, mring, step, eacc, total;
+  long long vol = 0, mon_cells = 0, n_mw = 0;
+  size_t fields, psi, zero_end, off[7], pts[7], mons, mw_off, mw, mring, step, eacc, total;
 };
+
+// Monitor boxes {comp, lo0, lo1, lo2, s0, s1, s2} in ring order: the listed
+// boxes, or the six full components when none are listed.
+static std::vector<std::array<int, 7>> mon_boxes3(const GdnYeeParams* p,
+                                                  const GdnYeePoints* pts) {
+  std::vector<std::array<int, 7>> v;
+  if (p->n_freq <= 0) return v;
+  if (p->n_monitors == 0) {
+    for (int c = 0; c < 6; ++c) {
+      int s[3];
+      comp_shape(c, p->nx, p->ny, p->nz, s);
+      v.push_back({c, 0, 0, 0, s[0], s[1], s[2]});
+    }
+    return v;
+  }
+  for (int k = 0; k < p->n_monitors; ++k) {
+    const GdnDftMonitor& g = pts->monitors[k];
+    v.push_back({g.comp, g.lo[0], g.lo[1], g.lo[2], g.hi[0] - g.lo[0], g.hi[1] - g.lo[1],
+                 g.hi[2] - g.lo[2]});
+  }
+  return v;
+}
+
+// (CTA, monitor) parts: every i-plane x (j, k) CTA tile a monitor box crosses.
+static long long mon_parts3(const GdnYeeParams* p, const GdnYeePoints* pts) {
+  long long n = 0;
+  for (const auto& b : mon_boxes3(p, pts))
+    if (b[4] > 0 && b[5] > 0 && b[6] > 0)
+      n += (long long)b[4] * ((b[2] + b[5] - 1) / BJ - b[2] / BJ + 1) *
+           ((b[3] + b[6] - 1) / BK - b[3] / BK + 1);
+  return n;
+}
 
 static long long mon_cells3(const GdnYeeParams* p, const GdnYeePoints* pts) {
   if (p->n_freq <= 0) return 0;
@@ -461,6 +537,7 @@ static Layout3 make_layout3(const GdnYeeParams* p, const GdnYeePoints* pts, size
   L.gj = int(div_up(p->ny, BJ));
   L.n_cta = p->nx * L.gj * L.gk;
   L.mon_cells = pts ? mon_cells3(p, pts) : 0;
+  L.n_mw = pts ? mon_parts3(p, pts) : 0;
   const size_t budget = size_t(2) << 30;
   long long r = L.mon_cells > 0 ? (long long)(budget / (size_t(L.mon_cells) * esize)) : 32;
   L.R = int(std::max<long long>(1, std::min<long long>(32, r)));
@@ -474,6 +551,8 @@ static Layout3 make_layout3(const GdnYeeParams* p, const GdnYeePoints* pts, size
     L.pts[t] = cv.take<Pt3>(std::max(count_of(p, t), 1));
   }
   L.mons = cv.take<Mon3>(std::max(p->n_monitors, 6));
+  L.mw_off = cv.take<int>(L.n_cta + 1);
+  L.mw = cv.take<MonW3>(size_t(std::max<long long>(L.n_mw, 1)));
   L.mring = cv.take<char>(std::max<size_t>(size_t(L.mon_cells) * L.R, 1) * esize);
   L.eacc = cv.take<double>(p->record_energy ? 2 * size_t(std::max(p->n_steps, 1)) : 1);
   L.total = cv.bytes();
@@ -559,7 +638,9 @@ static int validate3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYe
 template <typename T, typename A>
 static void launch_fold3(const Dev3<T>& d, const std::vector<Mon3>& mons, long long max_cells,
                          int cnt, int K, cudaStream_t s) {
-  const dim3 dg(unsigned(div_up(max_cells, 256)), unsigned(mons.size()));
+  (void)mons;
+  (void)max_cells;
+  const unsigned dg = unsigned(div_up(d.mon_cells, 256));
   const size_t sm = size_t(4) * cnt * K * sizeof(A);
   if (K <= 4)
     yee_fold<T, A, 4><<<dg, 256, sm, s>>>(d, cnt);
@@ -672,29 +753,58 @@ static int run3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuff
   const bool f64acc = p->dft_f64 != 0;
   const size_t csz = f64acc ? sizeof(double2) : sizeof(float2);
   std::vector<Mon3> mons;
-  if (p->n_freq > 0) {
+  {
     long long off = 0;
-    const int nm = p->n_monitors == 0 ? 6 : p->n_monitors;
-    for (int k = 0; k < nm; ++k) {
+    int k = 0;
+    for (const auto& bx : mon_boxes3(p, pts)) {
       Mon3 m{};
-      if (p->n_monitors == 0) {
-        int s[3];
-        comp_shape(k, nx, ny, nz, s);
-        m.comp = k;
-        m.s0 = s[0]; m.s1 = s[1]; m.s2 = s[2];
-        m.out = b->dft[k];
-      } else {
-        const GdnDftMonitor& g = pts->monitors[k];
-        m.comp = g.comp;
-        m.lo0 = g.lo[0]; m.lo1 = g.lo[1]; m.lo2 = g.lo[2];
-        m.s0 = g.hi[0] - g.lo[0]; m.s1 = g.hi[1] - g.lo[1]; m.s2 = g.hi[2] - g.lo[2];
-        m.out = g.out;
-      }
+      m.comp = bx[0];
+      m.lo0 = bx[1]; m.lo1 = bx[2]; m.lo2 = bx[3];
+      m.s0 = bx[4]; m.s1 = bx[5]; m.s2 = bx[6];
+      m.out = p->n_monitors == 0 ? b->dft[k] : pts->monitors[k].out;
       m.count = (long long)m.s0 * m.s1 * m.s2;
       m.off = off;
       off += m.count;
       mons.push_back(m);
+      ++k;
     }
+  }
+  // Monitor parts per CTA (CSR over CTA ids (i * gj + j / BJ) * gk + k / BK).
+  {
+    std::vector<int> cnt(L.n_cta + 1, 0);
+    auto for_parts = [&](auto&& fn) {
+      for (const Mon3& m : mons) {
+        if (m.count <= 0) continue;
+        for (int i = m.lo0; i < m.lo0 + m.s0; ++i)
+          for (int by = m.lo1 / BJ; by <= (m.lo1 + m.s1 - 1) / BJ; ++by)
+            for (int bx = m.lo2 / BK; bx <= (m.lo2 + m.s2 - 1) / BK; ++bx) {
+              MonW3 w{};
+              w.j0 = std::max(m.lo1, by * BJ);
+              w.j1 = std::min(m.lo1 + m.s1, (by + 1) * BJ);
+              w.k0 = std::max(m.lo2, bx * BK);
+              w.k1 = std::min(m.lo2 + m.s2, (bx + 1) * BK);
+              w.comp = m.comp;
+              w.s1 = m.s1;
+              w.s2 = m.s2;
+              w.base = m.off - ((long long)m.lo0 * m.s1 + m.lo1) * m.s2 - m.lo2;
+              fn((i * L.gj + by) * L.gk + bx, w);
+            }
+      }
+    };
+    for_parts([&](int c, const MonW3&) { cnt[c + 1]++; });
+    for (int c = 0; c < L.n_cta; ++c) cnt[c + 1] += cnt[c];
+    if ((long long)cnt[L.n_cta] != L.n_mw)
+      GDN_BAD_ARG("internal: %d monitor parts, layout sized for %lld", cnt[L.n_cta], L.n_mw);
+    std::vector<MonW3> mw(std::max<long long>(L.n_mw, 1));
+    std::vector<int> cur(cnt.begin(), cnt.end() - 1);
+    for_parts([&](int c, const MonW3& w) { mw[cur[c]++] = w; });
+    GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.mw_off, cnt.data(), cnt.size() * sizeof(int),
+                                 cudaMemcpyHostToDevice, stream));
+    if (L.n_mw > 0)
+      GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.mw, mw.data(), size_t(L.n_mw) * sizeof(MonW3),
+                                   cudaMemcpyHostToDevice, stream));
+    d.mw_off = reinterpret_cast<const int*>(ws + L.mw_off);
+    d.mw = reinterpret_cast<const MonW3*>(ws + L.mw);
   }
   d.n_mons = int(mons.size());
   d.mons = reinterpret_cast<const Mon3*>(ws + L.mons);
@@ -763,8 +873,10 @@ static int run3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuff
     return st;
   }
   cudaError_t le = cudaSuccess;
+  LoopTimer timer(stream, double(p->nx) * p->ny * p->nz * p->n_steps, p->n_steps);
   for (int c = 0; c < full && le == cudaSuccess; ++c) le = cudaGraphLaunch(g_full, stream);
   if (rem > 0 && le == cudaSuccess) le = cudaGraphLaunch(g_rem, stream);
+  timer.stop(le == cudaSuccess);
   if (g_full) cudaGraphExecDestroy(g_full);
   if (g_rem) cudaGraphExecDestroy(g_rem);
   if (le != cudaSuccess) {

@@ -138,3 +138,49 @@ def scatter_full(mon: RegionDFTMonitor, full_shapes):
             full[(slice(None),) + slab.slices()] = arr
         out.append(full)
     return DFTMonitor(mon.freqs, *out)
+
+
+# ---------------------------------------------------------------------------
+# Exact monitor boxes (several per component) for the 3D GdnDftMonitor list.
+# The reference's DFTRegions allow one bounding slab per component, which for
+# the NTFF box is the whole box volume; recording only the face layers that
+# ntff_3d reads gives the same phasors for a fraction of the DFT traffic.
+# A box is (comp, lo (3), hi (3)), half-open, in the component's indices.
+# ---------------------------------------------------------------------------
+
+
+def region_boxes(regions: DFTRegions):
+    """DFTRegions slabs as a box list."""
+    return [(c, tuple(s.lo), tuple(s.hi)) for c, s in enumerate(regions) if s is not None]
+
+
+def ntff_face_boxes(grid, box_margin):
+    """Every sample ntff_3d reads (src/gradenna/ntff.py:345-395): per face the
+    tangential E layer and the two tangential H layers around it."""
+    nx, ny, nz = grid.nx, grid.ny, grid.nz
+    m = int(box_margin)
+    i0, i1, j0, j1, k0, k1 = m, nx - 1 - m, m, ny - 1 - m, m, nz - 1 - m
+    out = []
+    for i in (i1, i0):
+        out += [(1, (i, j0, k0), (i + 1, j1, k1 + 1)), (2, (i, j0, k0), (i + 1, j1 + 1, k1)),
+                (4, (i - 1, j0, k0), (i + 1, j1 + 1, k1)), (5, (i - 1, j0, k0), (i + 1, j1, k1 + 1))]
+    for j in (j1, j0):
+        out += [(0, (i0, j, k0), (i1, j + 1, k1 + 1)), (2, (i0, j, k0), (i1 + 1, j + 1, k1)),
+                (3, (i0, j - 1, k0), (i1 + 1, j + 1, k1)), (5, (i0, j - 1, k0), (i1, j + 1, k1 + 1))]
+    for k in (k1, k0):
+        out += [(0, (i0, j0, k), (i1, j1 + 1, k + 1)), (1, (i0, j0, k), (i1 + 1, j1, k + 1)),
+                (3, (i0, j0, k - 1), (i1 + 1, j1, k + 1)), (4, (i0, j0, k - 1), (i1, j1 + 1, k + 1))]
+    return out
+
+
+def boxes_to_full(freqs, boxes, tensors, full_shapes):
+    """Zero-filled full-grid DFTMonitor from per-box spectra (n_freq, *box)."""
+    from gradenna_b200.fdtd3d import DFTMonitor
+
+    n_freq = freqs.shape[0]
+    dev = tensors[0].device if tensors else None
+    dt = tensors[0].dtype if tensors else torch.complex128
+    full = [torch.zeros((n_freq,) + tuple(s), dtype=dt, device=dev) for s in full_shapes]
+    for (c, lo, hi), t in zip(boxes, tensors):
+        full[c][(slice(None),) + tuple(slice(a, b) for a, b in zip(lo, hi))] = t
+    return DFTMonitor(freqs, *full)

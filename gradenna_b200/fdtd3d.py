@@ -59,6 +59,7 @@ class SimResult3D(NamedTuple):
     hx: torch.Tensor
     hy: torch.Tensor
     hz: torch.Tensor
+    monitors: list | None = None
 
 
 def field_energy_3d(ex, ey, ez, hx, hy, hz, eps, grid: Grid3D):
@@ -168,6 +169,7 @@ def simulate_3d(
     dft_freqs=None,
     dft_dtype=None,
     dft_regions=None,
+    dft_monitors=None,
     record_energy: bool = False,
     checkpoint_segments: int | None = None,
     dtype=None,
@@ -181,7 +183,9 @@ def simulate_3d(
     there (fdtd3d.py:738-741) and does not change the forward results.
     Additions: ``dtype``, ``device``, ``cw_sources`` = dict(env, src_w, jx_w,
     jy_w, mx_w, my_w, mz_w) for device-synthesised CW waveforms (the 3D
-    frequency-domain adjoint's drive).
+    frequency-domain adjoint's drive), and ``dft_monitors`` = [(comp, lo,
+    hi), ...] boxes (several per component allowed) whose spectra come back
+    as ``SimResult3D.monitors`` in the same order (``dft`` is then None).
     """
     nx, ny, nz = grid.nx, grid.ny, grid.nz
     if min(nx, ny, nz) <= 2 * cpml.thickness + 2:
@@ -349,7 +353,18 @@ def simulate_3d(
     regions = None
     mon_out = [None] * 6
     mons = []
-    if n_freq:
+    if dft_regions is not None and dft_monitors is not None:
+        raise ValueError("give dft_regions or dft_monitors, not both")
+    if n_freq and dft_monitors is not None:
+        for c, lo, hi in dft_monitors:
+            lo, hi = tuple(int(v) for v in lo), tuple(int(v) for v in hi)
+            if not 0 <= c < 6 or any(l < 0 or h > s or h <= l
+                                     for l, h, s in zip(lo, hi, shapes[c])):
+                raise ValueError(f"dft monitor {(c, lo, hi)} outside component {c}")
+            t = torch.empty((n_freq,) + tuple(h - l for l, h in zip(lo, hi)), dtype=cdt,
+                            device=dev)
+            mons.append((c, lo, hi, t))
+    elif n_freq:
         if dft_regions is None:
             mon_out = [torch.empty((n_freq,) + s, dtype=cdt, device=dev) for s in shapes]
         else:
@@ -369,9 +384,10 @@ def simulate_3d(
     prm.n_src, prm.n_jx, prm.n_jy = (chans[k][0].shape[0] for k in ("src", "jx", "jy"))
     prm.n_mx, prm.n_my, prm.n_mz = (chans[k][0].shape[0] for k in ("mx", "my", "mz"))
     prm.n_probes, prm.has_port = probe_idx.shape[0], int(has_port)
-    prm.n_freq = n_freq if (dft_regions is None or mons or cw) else 0
+    limited = dft_regions is not None or dft_monitors is not None
+    prm.n_freq = n_freq if (not limited or mons or cw) else 0
     prm.dft_f64 = int(cdt == torch.complex128)
-    prm.n_monitors = len(mons) if dft_regions is not None else 0
+    prm.n_monitors = len(mons) if limited else 0
     prm.record_energy, prm.cw_sources = int(bool(record_energy)), int(cw)
     prm.dt, prm.dx, prm.dy, prm.dz, prm.mu0 = dt, dx, dy, dz, MU0
 
@@ -401,7 +417,7 @@ def simulate_3d(
     bufs.out_v = _native.ptr(out_v)
     bufs.out_i = _native.ptr(out_i)
     bufs.out_energy = _native.ptr(out_e)
-    if n_freq and dft_regions is None:
+    if n_freq and not limited:
         for c in range(6):
             bufs.dft[c] = mon_out[c].data_ptr()
 
@@ -419,8 +435,13 @@ def simulate_3d(
     del keep
 
     dft = None
+    monitors = None
     if n_freq:
         ft = torch.as_tensor(freqs, device=dev)
-        dft = (DFTMonitor(ft, *mon_out) if dft_regions is None
-               else RegionDFTMonitor(ft, regions, *mon_out))
-    return SimResult3D(out_probe, out_v, out_i, out_e, dft, *fields)
+        if dft_monitors is not None:
+            monitors = [t for (_, _, _, t) in mons]
+        elif dft_regions is None:
+            dft = DFTMonitor(ft, *mon_out)
+        else:
+            dft = RegionDFTMonitor(ft, regions, *mon_out)
+    return SimResult3D(out_probe, out_v, out_i, out_e, dft, *fields, monitors)

@@ -53,10 +53,17 @@ class FreqPhasors3D(NamedTuple):
     port_i: torch.Tensor | None = None
 
 
-def _full_eps_sigma_3d(grid, design_sigma, design_eps_r, design_region, device):
-    """Vacuum background with the design values on design_region (freq_adjoint.py:611-617)."""
-    eps_r = torch.ones(grid.shape, dtype=torch.float64, device=device)
-    sigma = torch.zeros(grid.shape, dtype=torch.float64, device=device)
+def _full_eps_sigma_3d(grid, design_sigma, design_eps_r, design_region, device,
+                       eps_r_background=None, sigma_background=None):
+    """Background (vacuum unless given) with the design values on design_region
+    (freq_adjoint.py:611-617)."""
+    def bg(a, fill):
+        if a is None:
+            return torch.full(grid.shape, fill, dtype=torch.float64, device=device)
+        return torch.as_tensor(a, dtype=torch.float64, device=device).expand(grid.shape).clone()
+
+    eps_r = bg(eps_r_background, 1.0)
+    sigma = bg(sigma_background, 0.0)
     if design_eps_r is not None:
         eps_r[design_region] = torch.as_tensor(design_eps_r, dtype=torch.float64, device=device)
     if design_sigma is not None:
@@ -174,16 +181,23 @@ def freq_adjoint_gradient_3d(grid: Grid3D, objective, *, design_sigma=None, desi
                              port_ijk=None, port_voltage=None, port_resistance: float = 50.0,
                              cpml: CPMLSpec = CPMLSpec(), backend: str = "cuda",
                              objective_kind: str | None = None, box_margin: int | None = None,
-                             monitor_region=None, dtype=torch.float64, device=None):
+                             monitor_region=None, dtype=torch.float64, device=None,
+                             eps_r_background=None, sigma_background=None):
     """Two-run 3D frequency-domain adjoint gradient (freq_adjoint.py:864-1065).
 
     ``objective`` maps FreqPhasors3D (torch complex128 on the device) to a
     real scalar tensor; the source/port drive must be CW at ``dft_freqs``
     under the turn-on envelope ``env``. ``objective_kind`` ("port",
-    "ntff_box" or "field", with ``box_margin`` / ``monitor_region``) limits
-    the forward DFT to the design E slabs plus the objective's region and
-    the adjoint DFT to the design slabs, as in the reference; the gradient
-    is unchanged. ``backend`` is accepted for signature compatibility
+    "ntff_box" or "field", with ``box_margin`` / ``monitor_region``, or a
+    tuple of them) limits the forward DFT to the design E slabs plus what
+    the objective reads and the adjoint DFT to the design slabs, as in the
+    reference; the gradient is unchanged. Where the reference records one
+    bounding slab per component (for the NTFF box: the whole box volume),
+    this records exact boxes (for the NTFF box: the face layers ntff_3d
+    reads). ``eps_r_background`` / ``sigma_background`` (nx, ny, nz)
+    replace the reference's vacuum background (an addition: fixed structures
+    such as a substrate and ground plane around the design); the design
+    values overwrite them on design_region. ``backend`` is accepted for signature compatibility
     ("xla", "native", "cuda"); every run is the CUDA path. Returns
     {"sigma": ..., "eps_r": ...} (float64 tensors of the design shape) for
     the design variables supplied.
@@ -195,35 +209,47 @@ def freq_adjoint_gradient_3d(grid: Grid3D, objective, *, design_sigma=None, desi
     dev = _native.require_cuda(device)
     freqs = tuple(float(f) for f in dft_freqs)
     env = np.asarray(env.detach().cpu() if isinstance(env, torch.Tensor) else env, np.float64)
-    eps_r, sigma = _full_eps_sigma_3d(grid, design_sigma, design_eps_r, design_region, dev)
+    eps_r, sigma = _full_eps_sigma_3d(grid, design_sigma, design_eps_r, design_region, dev,
+                                      eps_r_background, sigma_background)
     shapes = dr.full_field_shapes(grid.nx, grid.ny, grid.nz)
 
-    fwd_regions = adj_regions = None
+    # Region-limited DFT: exact monitor boxes (the design E slabs, plus what
+    # the objective reads in the forward run). The objective and the
+    # contraction see zero-filled full grids, so the gradient is unchanged.
+    fwd_boxes = adj_boxes = None
     if objective_kind is not None:
-        adj_regions = dr.design_region_to_slabs(design_region, shapes)
-        if objective_kind == "port":
-            if port_ijk is None:
-                raise ValueError("objective_kind='port' requires port_ijk")
-            obj_regions = dr.port_regions(port_ijk, shapes)
-        elif objective_kind == "ntff_box":
-            if box_margin is None:
-                raise ValueError("objective_kind='ntff_box' requires box_margin")
-            obj_regions = dr.ntff_box_regions(grid, box_margin, shapes)
-        elif objective_kind == "field":
-            if monitor_region is None:
-                raise ValueError("objective_kind='field' requires monitor_region")
-            obj_regions = dr.field_regions(monitor_region, shapes)
-        else:
-            raise ValueError("objective_kind must be 'port', 'ntff_box' or 'field', "
-                             f"got {objective_kind!r}")
-        fwd_regions = dr.union_regions(adj_regions, obj_regions)
+        kinds = (objective_kind,) if isinstance(objective_kind, str) else tuple(objective_kind)
+        adj_boxes = dr.region_boxes(dr.design_region_to_slabs(design_region, shapes))
+        fwd_boxes = list(adj_boxes)
+        for kind in kinds:
+            if kind == "port":
+                if port_ijk is None:
+                    raise ValueError("objective_kind='port' requires port_ijk")
+                fwd_boxes += dr.region_boxes(dr.port_regions(port_ijk, shapes))
+            elif kind == "ntff_box":
+                if box_margin is None:
+                    raise ValueError("objective_kind='ntff_box' requires box_margin")
+                fwd_boxes += dr.ntff_face_boxes(grid, box_margin)
+            elif kind == "field":
+                if monitor_region is None:
+                    raise ValueError("objective_kind='field' requires monitor_region")
+                fwd_boxes += dr.region_boxes(dr.field_regions(monitor_region, shapes))
+            else:
+                raise ValueError("objective_kind must be 'port', 'ntff_box' or 'field' (or a "
+                                 f"tuple of them), got {kind!r}")
+
+    def phasors(res, boxes):
+        if boxes is None:
+            return res.dft
+        ft = torch.as_tensor(np.asarray(freqs), device=dev)
+        return dr.boxes_to_full(ft, boxes, res.monitors, shapes)
 
     common = dict(eps_r=eps_r, sigma=sigma, dft_freqs=freqs, dft_dtype=np.complex128, cpml=cpml,
                   dtype=dtype, device=dev)
     fwd = simulate_3d(grid, source_ijk=source_ijk, source_current=source_current,
                       port_ijk=port_ijk, port_voltage=port_voltage,
-                      port_resistance=port_resistance, dft_regions=fwd_regions, **common)
-    fd = _full_phasors(fwd, grid)
+                      port_resistance=port_resistance, dft_monitors=fwd_boxes, **common)
+    fd = phasors(fwd, fwd_boxes)
     comps = [fd.ex, fd.ey, fd.ez, fd.hx, fd.hy, fd.hz]
 
     # Objective cotangents; torch's complex gradient is the conjugate of jax's.
@@ -254,8 +280,8 @@ def freq_adjoint_gradient_3d(grid: Grid3D, objective, *, design_sigma=None, desi
     for key, (idx, w) in chans.items():
         kw[names[key][0]] = idx
         cw[f"{key}_w"] = w
-    adj = simulate_3d(grid, dft_regions=adj_regions, cw_sources=cw, **kw, **common)
-    ad = _full_phasors(adj, grid)
+    adj = simulate_3d(grid, dft_monitors=adj_boxes, cw_sources=cw, **kw, **common)
+    ad = phasors(adj, adj_boxes)
 
     sel = (slice(None),) + tuple(design_region)
     eps_d, sig_d = eps_r[design_region], sigma[design_region]

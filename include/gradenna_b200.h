@@ -64,15 +64,16 @@ const char* gdn_last_error(void);
  * counterpart: it lets callers and benchmarks attribute device work. */
 uint64_t gdn_kernel_launches(void);
 
-/* Device time of the 2D time loops run since the last reset. Every
- * gdn_tm_run_f32/f64 records CUDA events on its stream around the replay of
- * its time loop (the TB-step block launches, DFT folds and step-counter
- * advances); this call waits for those events and returns the summed
- * milliseconds, the summed nx*ny*n_steps and the number of blocks (one
- * block = one TB-step launch of the whole grid), then forgets the records
- * when reset != 0. At most 4096 runs are recorded between resets. No
- * reference counterpart: it gives benchmarks a per-launch kernel time
- * measured inside their own timed region. */
+/* Device time of the time loops run since the last reset. Every
+ * gdn_tm_run_f32/f64 and gdn_yee_run_f32/f64 records CUDA events on its
+ * stream around the replay of its time loop (the step kernels, DFT folds and
+ * step-counter advances); this call waits for those events and returns the
+ * summed milliseconds, the summed cells x n_steps and the number of blocks
+ * (2D: one block = one TB-step launch of the whole grid; 3D: one block = one
+ * time step), then forgets the records when reset != 0. At most 4096 runs
+ * are recorded between resets. No reference counterpart: it gives
+ * benchmarks a per-launch kernel time measured inside their own timed
+ * region. */
 int gdn_tm_loop_stats(double* loop_ms, double* cell_steps, int64_t* blocks, int32_t reset);
 
 /* ------------------------------------------------------------------------ */
