@@ -41,6 +41,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <mutex>
+#include <type_traits>
 #include <vector>
 
 #include "common.cuh"
@@ -58,10 +59,16 @@ constexpr int MAXP = 64;  // most port records in one tile
 struct Cfg {
   int tb, ti, tj, nt;
 };
-// Per field type three TB=4 shapes, largest first (pick_cfg chooses one from
-// the grid size; GDN_TM_TILE=0/1/2 forces one, for tuning). The one-step shape serves runs that record the energy every step.
-constexpr Cfg kCfgF32[3] = {{4, 64, 64, 512}, {4, 32, 64, 256}, {4, 16, 32, 128}};
-constexpr Cfg kCfgF64[3] = {{4, 28, 64, 512}, {4, 16, 64, 256}, {4, 16, 32, 128}};
+// Per field type five shapes: three with TB = 4 (largest first) and two
+// with TB = 2. pick_cfg chooses a TB = 4 one from the grid size;
+// GDN_TM_TILE=0..4 or the batched entry point's `cfg` argument (set by the
+// autotuner) forces any. The one-step shape serves runs that record the
+// energy every step.
+constexpr int NCFG = 5;
+constexpr Cfg kCfgF32[NCFG] = {
+    {4, 64, 64, 512}, {4, 32, 64, 256}, {4, 16, 32, 128}, {2, 64, 64, 512}, {2, 32, 64, 256}};
+constexpr Cfg kCfgF64[NCFG] = {
+    {4, 28, 64, 512}, {4, 16, 64, 256}, {4, 16, 32, 128}, {2, 28, 64, 512}, {2, 16, 64, 256}};
 constexpr Cfg kCfgStep{1, 16, 64, 256};  // one step per launch (energy records)
 
 struct Pt {
@@ -318,7 +325,7 @@ __device__ __forceinline__ void st16(T* dst, const T* src) {
 // no masks. Both sweep 16-byte vectors of cells along a row.
 // ---------------------------------------------------------------------------
 template <typename T, int TB, int TI, int TJ, int NT, bool GEN>
-__global__ void __launch_bounds__(NT) tm_tb(Dev<T> d, const int* tiles, int sub0, int nsub) {
+__device__ __forceinline__ void tb_body(const Dev<T>& d, const int tile, int sub0, int nsub) {
   constexpr int EH = TI + 2 * TB;  // extended rows
   constexpr int EW = TJ + 2 * HJ;  // extended columns
   constexpr int EC = EH * EW;
@@ -337,7 +344,6 @@ __global__ void __launch_bounds__(NT) tm_tb(Dev<T> d, const int* tiles, int sub0
   const int n0 = *d.step_base + sub0;
   const int par = (n0 / TB) & 1;
   const int nx = d.nx, ny = d.ny, ld = d.ld, npml = d.npml;
-  const int tile = tiles[blockIdx.x];
   const int ty = tile / d.tiles_x, tx = tile - ty * d.tiles_x;
   const int i0 = ty * TI, j0 = tx * TJ;
   const int ie = i0 - TB, je = j0 - HJ;  // global cell of extended (0, 0)
@@ -547,6 +553,26 @@ __global__ void __launch_bounds__(NT) tm_tb(Dev<T> d, const int* tiles, int sub0
   }
 }
 
+template <typename T, int TB, int TI, int TJ, int NT, bool GEN>
+__global__ void __launch_bounds__(NT) tm_tb(Dev<T> d, const int* tiles, int sub0, int nsub) {
+  tb_body<T, TB, TI, TJ, NT, GEN>(d, tiles[blockIdx.x], sub0, nsub);
+}
+
+// Batched form: CTA b runs tile work[b].y of problem work[b].x, whose run
+// description is copied from global memory into shared memory first. All
+// problems of one launch share the tile shape, TB, sub0 and nsub.
+template <typename T, int TB, int TI, int TJ, int NT, bool GEN>
+__global__ void __launch_bounds__(NT) tm_tb_batch(const Dev<T>* devs, const int2* work, int sub0,
+                                                  int nsub) {
+  __shared__ __align__(16) unsigned char sdev[sizeof(Dev<T>)];
+  const int2 w = work[blockIdx.x];
+  const int* srcw = reinterpret_cast<const int*>(devs + w.x);
+  for (int q = threadIdx.x; q < int(sizeof(Dev<T>) / sizeof(int)); q += NT)
+    reinterpret_cast<int*>(sdev)[q] = srcw[q];
+  __syncthreads();
+  tb_body<T, TB, TI, TJ, NT, GEN>(*reinterpret_cast<const Dev<T>*>(sdev), w.y, sub0, nsub);
+}
+
 // ---------------------------------------------------------------------------
 // Running DFT fold over `cnt` monitor-ring slots (fdtd2d.py:453-458): for
 // each monitored cell, acc_k += sum_t ph[n0+t, k] x_t, partial sums in A.
@@ -735,11 +761,12 @@ struct Layout {
 
 // Tile shape: one step per launch when the energy is recorded, else the
 // largest TB=4 shape that still yields two CTAs per SM's worth of tiles.
-static Cfg pick_cfg(const GdnTmParams* p, size_t esize) {
+static Cfg pick_cfg(const GdnTmParams* p, size_t esize, int force = -1) {
   if (p->record_energy) return kCfgStep;
   const Cfg* c = esize == sizeof(float) ? kCfgF32 : kCfgF64;
+  if (force >= 0 && force < NCFG) return c[force];
   const char* env = getenv("GDN_TM_TILE");
-  if (env && env[0] >= '0' && env[0] <= '2' && env[1] == 0) return c[env[0] - '0'];
+  if (env && env[0] >= '0' && env[0] < '0' + NCFG && env[1] == 0) return c[env[0] - '0'];
   // Measured on B200 (f32): 64x64 tiles win once they give every SM a tile
   // (1024^2: 129 vs 119/125 Gcell-steps/s); below that the 16x32 tiles keep
   // more SMs busy (512^2: 47 vs 34; 140^2: 5.1 vs 2.7).
@@ -795,9 +822,9 @@ static bool tile_is_interior(const GdnTmParams* p, const Cfg& c, int ty, int tx)
 
 // `ring_steps` > 0 forces the monitor-ring length (a multiple of TB).
 static Layout make_layout(const GdnTmParams* p, const GdnTmPoints* pts, size_t esize,
-                          int ring_steps = 0) {
+                          int ring_steps = 0, int force_cfg = -1) {
   Layout L;
-  L.cfg = pick_cfg(p, esize);
+  L.cfg = pick_cfg(p, esize, force_cfg);
   const Cfg& c = L.cfg;
   L.tiles_x = int(div_up(p->ny, c.tj));
   L.tiles_y = int(div_up(p->nx, c.ti));
@@ -985,24 +1012,35 @@ static size_t tb_smem() {
   return size_t(GEN ? 9 : 5) * (TI + 2 * TB) * (TJ + 2 * HJ) * sizeof(T);
 }
 
-// Per-type tile configurations: TB-step kernel and one-step kernel.
+// Per-type tile configurations (compile-time copies of the tables).
 template <typename T>
 struct Kern;
 template <>
 struct Kern<float> {
-  static constexpr Cfg c0 = kCfgF32[0], c1 = kCfgF32[1], c2 = kCfgF32[2];
+  static constexpr const Cfg* c = kCfgF32;
 };
 template <>
 struct Kern<double> {
-  static constexpr Cfg c0 = kCfgF64[0], c1 = kCfgF64[1], c2 = kCfgF64[2];
+  static constexpr const Cfg* c = kCfgF64;
 };
 
 template <typename T, int TB, int TI, int TJ, int NT, bool GEN>
 static int set_attr() {
+  const int sm = int(tb_smem<T, TB, TI, TJ, GEN>());
   GDN_TRY_CUDA(cudaFuncSetAttribute(tm_tb<T, TB, TI, TJ, NT, GEN>,
-                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                    int(tb_smem<T, TB, TI, TJ, GEN>())));
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
+  if constexpr (std::is_same<T, float>::value && TB > 1)
+    GDN_TRY_CUDA(cudaFuncSetAttribute(tm_tb_batch<T, TB, TI, TJ, NT, GEN>,
+                                      cudaFuncAttributeMaxDynamicSharedMemorySize, sm));
   return GDN_OK;
+}
+
+template <typename T, int I>
+static int set_attr_cfg() {
+  constexpr Cfg C = I < NCFG ? Kern<T>::c[I < NCFG ? I : 0] : kCfgStep;
+  int st;
+  if ((st = set_attr<T, C.tb, C.ti, C.tj, C.nt, true>())) return st;
+  return set_attr<T, C.tb, C.ti, C.tj, C.nt, false>();
 }
 
 template <typename T>
@@ -1010,17 +1048,21 @@ static int set_kernel_attributes() {
   static bool done = false;  // per process; the attribute is per function
   if (done) return GDN_OK;
   int st;
-  constexpr Cfg A = Kern<T>::c0, B = Kern<T>::c1, C = Kern<T>::c2, S = kCfgStep;
-  if ((st = set_attr<T, A.tb, A.ti, A.tj, A.nt, true>())) return st;
-  if ((st = set_attr<T, A.tb, A.ti, A.tj, A.nt, false>())) return st;
-  if ((st = set_attr<T, B.tb, B.ti, B.tj, B.nt, true>())) return st;
-  if ((st = set_attr<T, B.tb, B.ti, B.tj, B.nt, false>())) return st;
-  if ((st = set_attr<T, C.tb, C.ti, C.tj, C.nt, true>())) return st;
-  if ((st = set_attr<T, C.tb, C.ti, C.tj, C.nt, false>())) return st;
-  if ((st = set_attr<T, S.tb, S.ti, S.tj, S.nt, true>())) return st;
-  if ((st = set_attr<T, S.tb, S.ti, S.tj, S.nt, false>())) return st;
+  if ((st = set_attr_cfg<T, 0>()) || (st = set_attr_cfg<T, 1>()) || (st = set_attr_cfg<T, 2>()) ||
+      (st = set_attr_cfg<T, 3>()) || (st = set_attr_cfg<T, 4>()) || (st = set_attr_cfg<T, NCFG>()))
+    return st;
   done = true;
   return GDN_OK;
+}
+
+// Index of a run's configuration in its type's table (NCFG: the one-step shape).
+template <typename T>
+static int cfg_index(const Cfg& c) {
+  if (c.tb == 1) return NCFG;
+  for (int i = 0; i < NCFG; ++i)
+    if (Kern<T>::c[i].tb == c.tb && Kern<T>::c[i].ti == c.ti && Kern<T>::c[i].tj == c.tj)
+      return i;
+  return 0;
 }
 
 template <typename T, int TB, int TI, int TJ, int NT, bool GEN>
@@ -1030,14 +1072,32 @@ static void launch_cfg(const Run<T>& R, const int* tiles, int count, int sub0, i
       <<<count, NT, tb_smem<T, TB, TI, TJ, GEN>(), s>>>(R.d, tiles, sub0, nsub);
 }
 
+template <typename T, int I, bool GEN>
+static void launch_idx(const Run<T>& R, const int* tiles, int count, int sub0, int nsub,
+                       cudaStream_t s) {
+  constexpr Cfg C = I < NCFG ? Kern<T>::c[I < NCFG ? I : 0] : kCfgStep;
+  launch_cfg<T, C.tb, C.ti, C.tj, C.nt, GEN>(R, tiles, count, sub0, nsub, s);
+}
+
+template <typename T, bool GEN>
+static void launch_which(int which, const Run<T>& R, const int* tiles, int count, int sub0,
+                         int nsub, cudaStream_t s) {
+  switch (which) {
+    case 0: launch_idx<T, 0, GEN>(R, tiles, count, sub0, nsub, s); break;
+    case 1: launch_idx<T, 1, GEN>(R, tiles, count, sub0, nsub, s); break;
+    case 2: launch_idx<T, 2, GEN>(R, tiles, count, sub0, nsub, s); break;
+    case 3: launch_idx<T, 3, GEN>(R, tiles, count, sub0, nsub, s); break;
+    case 4: launch_idx<T, 4, GEN>(R, tiles, count, sub0, nsub, s); break;
+    default: launch_idx<T, NCFG, GEN>(R, tiles, count, sub0, nsub, s); break;
+  }
+}
+
 // Launch the general and the interior tiles for `nsub` steps starting at
 // chunk offset `sub0`; with a side stream the two run concurrently.
 template <typename T>
 static uint64_t launch_tb(const Run<T>& R, int sub0, int nsub, cudaStream_t s, cudaStream_t side,
                           cudaEvent_t fork, cudaEvent_t join) {
-  constexpr Cfg A = Kern<T>::c0, B = Kern<T>::c1, C = Kern<T>::c2, S = kCfgStep;
-  const Cfg& c = R.L.cfg;
-  const int which = c.tb == 1 ? 3 : (c.ti == A.ti && c.tj == A.tj ? 0 : (c.ti == B.ti && c.tj == B.tj ? 1 : 2));
+  const int which = cfg_index<T>(R.L.cfg);
   const int ng = R.L.n_gen, ni = R.L.n_int;
   cudaStream_t si = s;
   if (side && ng > 0 && ni > 0) {
@@ -1046,27 +1106,14 @@ static uint64_t launch_tb(const Run<T>& R, int sub0, int nsub, cudaStream_t s, c
     si = side;
   }
   uint64_t k = 0;
-#define GDN_LAUNCH(CF, GEN, TL, CNT, ST) \
-  launch_cfg<T, CF.tb, CF.ti, CF.tj, CF.nt, GEN>(R, TL, CNT, sub0, nsub, ST)
   if (ng > 0) {
-    switch (which) {
-      case 0: GDN_LAUNCH(A, true, R.tiles, ng, s); break;
-      case 1: GDN_LAUNCH(B, true, R.tiles, ng, s); break;
-      case 2: GDN_LAUNCH(C, true, R.tiles, ng, s); break;
-      default: GDN_LAUNCH(S, true, R.tiles, ng, s); break;
-    }
+    launch_which<T, true>(which, R, R.tiles, ng, sub0, nsub, s);
     ++k;
   }
   if (ni > 0) {
-    switch (which) {
-      case 0: GDN_LAUNCH(A, false, R.tiles + ng, ni, si); break;
-      case 1: GDN_LAUNCH(B, false, R.tiles + ng, ni, si); break;
-      case 2: GDN_LAUNCH(C, false, R.tiles + ng, ni, si); break;
-      default: GDN_LAUNCH(S, false, R.tiles + ng, ni, si); break;
-    }
+    launch_which<T, false>(which, R, R.tiles + ng, ni, sub0, nsub, si);
     ++k;
   }
-#undef GDN_LAUNCH
   if (si != s) {
     cudaEventRecord(join, side);
     cudaStreamWaitEvent(s, join, 0);
@@ -1412,6 +1459,203 @@ static int run(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuffers*
   return finalize(p, b, R, stream);
 }
 
+
+// ---------------------------------------------------------------------------
+// Batched runs: many independent problems advanced by shared launches.
+// ---------------------------------------------------------------------------
+
+template <int I>
+static void launch_batch_idx(bool gen, const Dev<float>* devs, const int2* work, int count,
+                             int sub0, int nsub, cudaStream_t s) {
+  constexpr Cfg C = kCfgF32[I];
+  if (gen)
+    tm_tb_batch<float, C.tb, C.ti, C.tj, C.nt, true>
+        <<<count, C.nt, tb_smem<float, C.tb, C.ti, C.tj, true>(), s>>>(devs, work, sub0, nsub);
+  else
+    tm_tb_batch<float, C.tb, C.ti, C.tj, C.nt, false>
+        <<<count, C.nt, tb_smem<float, C.tb, C.ti, C.tj, false>(), s>>>(devs, work, sub0, nsub);
+}
+
+static void launch_batch(int which, bool gen, const Dev<float>* devs, const int2* work, int count,
+                         int sub0, int nsub, cudaStream_t s) {
+  switch (which) {
+    case 0: launch_batch_idx<0>(gen, devs, work, count, sub0, nsub, s); break;
+    case 1: launch_batch_idx<1>(gen, devs, work, count, sub0, nsub, s); break;
+    case 2: launch_batch_idx<2>(gen, devs, work, count, sub0, nsub, s); break;
+    case 3: launch_batch_idx<3>(gen, devs, work, count, sub0, nsub, s); break;
+    default: launch_batch_idx<4>(gen, devs, work, count, sub0, nsub, s); break;
+  }
+}
+
+// All problems share one tile configuration (`cfg`, or the heuristic for the
+// largest problem) and one monitor-ring length, so chunk boundaries line up;
+// each keeps its own grid, CPML, sources, ports, monitors and step count.
+// Per block launch the work list holds (problem, tile) pairs of the problems
+// still running, ordered by decreasing step count so the active ones are a
+// prefix; a problem whose last block is partial gets its own launch.
+static int run_batch_f32(const GdnTmProblem* probs, int n, int cfg, cudaStream_t stream) {
+  using T = float;
+  if (n < 0 || (n > 0 && !probs)) GDN_BAD_ARG("invalid problem list");
+  if (cfg < -1 || cfg >= NCFG) GDN_BAD_ARG("cfg %d outside [-1, %d)", cfg, NCFG);
+  if (n == 0) return GDN_OK;
+  int st;
+  if ((st = set_kernel_attributes<T>())) return st;
+  // Configuration and common ring length.
+  int big = 0;
+  for (int q = 0; q < n; ++q) {
+    const GdnTmProblem& pr = probs[q];
+    if ((st = validate(pr.params, pr.points, pr.buffers))) {
+      const std::string msg = last_error();
+      GDN_BAD_ARG("problem %d: %s", q, msg.c_str());
+    }
+    if (pr.params->record_energy) GDN_BAD_ARG("problem %d: batched runs do not record the energy", q);
+    const GdnTmParams* a = pr.params;
+    const GdnTmParams* b0 = probs[big].params;
+    if ((long long)a->nx * a->ny > (long long)b0->nx * b0->ny) big = q;
+  }
+  const int which = cfg >= 0 ? cfg : cfg_index<T>(pick_cfg(probs[big].params, sizeof(T)));
+  std::vector<Run<T>> R(n);
+  int ring = 1 << 30;
+  for (int q = 0; q < n; ++q) {
+    R[q].L = make_layout(probs[q].params, probs[q].points, sizeof(T), 0, which);
+    ring = std::min(ring, R[q].L.R);
+  }
+  const int tb = kCfgF32[which].tb;
+  // Workspaces (the caller's, or one stream-ordered block for the rest) and
+  // a device block for the run descriptors and work lists.
+  std::vector<size_t> woff(n, 0);
+  size_t own_bytes = 0;
+  for (int q = 0; q < n; ++q) {
+    if (R[q].L.R != ring)
+      R[q].L = make_layout(probs[q].params, probs[q].points, sizeof(T), ring, which);
+    const GdnTmBuffers* b = probs[q].buffers;
+    if (b->workspace) {
+      if (b->workspace_bytes < R[q].L.total)
+        GDN_BAD_ARG("problem %d: workspace too small: %zu < %zu bytes", q, b->workspace_bytes,
+                    R[q].L.total);
+    } else {
+      woff[q] = own_bytes;
+      own_bytes += (R[q].L.total + 255) & ~size_t(255);
+    }
+  }
+  // Order by decreasing step count; work lists per tile class.
+  std::vector<int> order(n);
+  for (int q = 0; q < n; ++q) order[q] = q;
+  std::stable_sort(order.begin(), order.end(), [&](int u, int v) {
+    return probs[u].params->n_steps > probs[v].params->n_steps;
+  });
+  std::vector<int2> wgen, wint;
+  std::vector<int> gpos(n + 1, 0), ipos(n + 1, 0);  // prefix positions in `order` order
+  for (int r = 0; r < n; ++r) {
+    const int q = order[r];
+    const GdnTmParams* p = probs[q].params;
+    const Layout& L = R[q].L;
+    gpos[r] = int(wgen.size());
+    ipos[r] = int(wint.size());
+    for (int ty = 0; ty < L.tiles_y; ++ty)
+      for (int tx = 0; tx < L.tiles_x; ++tx)
+        (tile_is_interior(p, L.cfg, ty, tx) ? wint : wgen).push_back(make_int2(q, ty * L.tiles_x + tx));
+  }
+  gpos[n] = int(wgen.size());
+  ipos[n] = int(wint.size());
+  const size_t dev_bytes = size_t(n) * sizeof(Dev<T>);
+  const size_t aux = ((dev_bytes + 255) & ~size_t(255)) + (wgen.size() + wint.size() + 2) * sizeof(int2);
+  char* block = nullptr;
+  GDN_TRY_CUDA(cudaMallocAsync(reinterpret_cast<void**>(&block), own_bytes + aux + 256, stream));
+  struct Guard {
+    char* p;
+    cudaStream_t s;
+    ~Guard() {
+      if (p) cudaFreeAsync(p, s);
+    }
+  } guard{block, stream};
+  char* aux_base = block + ((own_bytes + 255) & ~size_t(255));
+  Dev<T>* d_devs = reinterpret_cast<Dev<T>*>(aux_base);
+  int2* d_gen = reinterpret_cast<int2*>(aux_base + ((dev_bytes + 255) & ~size_t(255)));
+  int2* d_int = d_gen + wgen.size() + 1;
+  // Prepare every problem in its workspace.
+  std::vector<Dev<T>> hdev(n);
+  for (int q = 0; q < n; ++q) {
+    const GdnTmBuffers* b = probs[q].buffers;
+    char* ws = b->workspace ? static_cast<char*>(b->workspace) : block + woff[q];
+    if ((st = prepare(probs[q].params, probs[q].points, b, ws, R[q], stream))) {
+      const std::string msg = last_error();
+      GDN_BAD_ARG("problem %d: %s", q, msg.c_str());
+    }
+    hdev[q] = R[q].d;
+  }
+  GDN_TRY_CUDA(cudaMemcpyAsync(d_devs, hdev.data(), dev_bytes, cudaMemcpyHostToDevice, stream));
+  if (!wgen.empty())
+    GDN_TRY_CUDA(cudaMemcpyAsync(d_gen, wgen.data(), wgen.size() * sizeof(int2),
+                                 cudaMemcpyHostToDevice, stream));
+  if (!wint.empty())
+    GDN_TRY_CUDA(cudaMemcpyAsync(d_int, wint.data(), wint.size() * sizeof(int2),
+                                 cudaMemcpyHostToDevice, stream));
+  // The host arrays above are pageable: cudaMemcpyAsync has staged them when
+  // it returns, so the vectors may be reused below.
+  int nmax = 0;
+  double cell_steps = 0;
+  int64_t blocks = 0;
+  for (int q = 0; q < n; ++q) {
+    const GdnTmParams* p = probs[q].params;
+    nmax = std::max(nmax, p->n_steps);
+    cell_steps += double(p->nx) * p->ny * p->n_steps;
+    blocks += div_up(p->n_steps, tb);
+  }
+  uint64_t launches = 0;
+  LoopTimer timer(stream, cell_steps, blocks);
+  auto launch_range = [&](int r0, int r1, int sub, int nsub) {
+    const int g0 = gpos[r0], g1 = gpos[r1], i0 = ipos[r0], i1 = ipos[r1];
+    if (g1 > g0) {
+      launch_batch(which, true, d_devs, d_gen + g0, g1 - g0, sub, nsub, stream);
+      ++launches;
+    }
+    if (i1 > i0) {
+      launch_batch(which, false, d_devs, d_int + i0, i1 - i0, sub, nsub, stream);
+      ++launches;
+    }
+  };
+  for (int base = 0; base < nmax; base += ring) {
+    for (int sub = 0; sub < ring && base + sub < nmax; sub += tb) {
+      // Problems with a full block here form a prefix of `order`.
+      int full = 0;
+      while (full < n && probs[order[full]].params->n_steps - base - sub >= tb) ++full;
+      launch_range(0, full, sub, tb);
+      // Then the problems whose last block this is, one launch each.
+      for (int r = full; r < n; ++r) {
+        const int left = probs[order[r]].params->n_steps - base - sub;
+        if (left <= 0) break;
+        launch_range(r, r + 1, sub, left);
+      }
+    }
+    for (int r = 0; r < n; ++r) {
+      const int q = order[r];
+      const GdnTmParams* p = probs[q].params;
+      const int cnt = std::min(ring, p->n_steps - base);
+      if (cnt <= 0) break;
+      if (!R[q].mons.empty()) {
+        if (p->dft_f64)
+          launch_fold<T, double>(R[q], cnt, p->n_freq, stream);
+        else
+          launch_fold<T, float>(R[q], cnt, p->n_freq, stream);
+        ++launches;
+      }
+      tm_advance<<<1, 1, 0, stream>>>(R[q].step_base, cnt);
+      ++launches;
+    }
+  }
+  const cudaError_t le = cudaGetLastError();
+  timer.stop(le == cudaSuccess);
+  if (le != cudaSuccess) {
+    set_error("batched launch failed: %s", cudaGetErrorString(le));
+    return GDN_ERR_CUDA;
+  }
+  count_launches(launches);
+  for (int q = 0; q < n; ++q)
+    if ((st = finalize(probs[q].params, probs[q].buffers, R[q], stream))) return st;
+  return GDN_OK;
+}
+
 }  // namespace tm2d
 }  // namespace gdn
 
@@ -1436,6 +1680,11 @@ extern "C" int gdn_tm_workspace_size(const GdnTmParams* p, const GdnTmPoints* pt
 extern "C" int gdn_tm_run_f32(const GdnTmParams* p, const GdnTmPoints* pts,
                               const GdnTmBuffers* b, void* stream) {
   return gdn::tm2d::run<float>(p, pts, b, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int gdn_tm_run_batch_f32(const GdnTmProblem* problems, int32_t n, int32_t cfg,
+                                    void* stream) {
+  return gdn::tm2d::run_batch_f32(problems, n, cfg, static_cast<cudaStream_t>(stream));
 }
 
 extern "C" int gdn_tm_run_f64(const GdnTmParams* p, const GdnTmPoints* pts,

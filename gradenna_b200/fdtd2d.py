@@ -168,7 +168,7 @@ def _region_rect(r, shape):
     return (lo0, lo1, hi0, hi1)
 
 
-def simulate_tm(
+def _prepare_tm(
     grid: Grid2D,
     *,
     source_ij=None,
@@ -190,26 +190,10 @@ def simulate_tm(
     dft_region=None,
     dft_monitors=None,
     cw_sources=None,
-) -> SimResult:
-    """Run a 2D TM FDTD simulation on the GPU (drop-in for fdtd2d.simulate_tm).
-
-    Arguments and semantics follow the reference (fdtd2d.py:181-247):
-    ``source_ij``/``source_current`` Jz line currents sampled at (n+1/2) dt;
-    ``eps_r``/``sigma`` scalars or (nx, ny); ``probe_ij`` Ez probes;
-    ``ports`` lumped RVS ports; ``dft_freqs`` running-DFT frequencies with
-    ``dft_dtype`` accumulators (default complex64 for float32 fields);
-    ``cpml``; ``record_energy``; ``mx_*``/``my_*`` magnetic currents on the
-    Hx/Hy grids injected as H -= (dt/mu) M.
-
-    Additions: ``dtype`` forces the field dtype; ``device`` selects the CUDA
-    device; ``dft_region`` = (ez_rect, hx_rect, hy_rect), each
-    (lo_i, lo_j, hi_i, hi_j) or None, limits the DFT to those rectangles;
-    ``dft_monitors`` = [(comp, lo_i, lo_j, hi_i, hi_j), ...] with comp 0/1/2 =
-    ez/hx/hy records only those boxes (returned in ``SimResult.monitors``,
-    dft_ez/hx/hy are then None); ``cw_sources`` = dict(env, src_w, mx_w, my_w) synthesises the Jz/Mx/My
-    waveforms on the device as env[n] Re(sum_k W_k exp(+i w_k t_n)) (the
-    frequency-domain adjoint's CW drive) instead of reading tabulated ones.
-    """
+) -> "_Prep":
+    """Validate the arguments of simulate_tm and build its C-ABI structs,
+    device inputs and output tensors (everything but the workspace and the
+    call)."""
     nx, ny = grid.nx, grid.ny
     if min(nx, ny) <= 2 * cpml.thickness + 2:
         raise ValueError(f"grid {nx}x{ny} is too small for CPML thickness {cpml.thickness}")
@@ -465,25 +449,10 @@ def simulate_tm(
     bufs.out_energy = _native.ptr(out_energy)
     bufs.dft_ez, bufs.dft_hx, bufs.dft_hy = (_native.ptr(t) for t in dft_out)
 
-    f64 = fdt == torch.float64
-    nbytes = ctypes.c_size_t(0)
-    _native.check(lib.gdn_tm_workspace_size(ctypes.byref(params), ctypes.byref(pts), int(f64),
-                                            ctypes.byref(nbytes)))
-    ws = torch.empty(max(int(nbytes.value), 1), dtype=torch.uint8, device=dev)
-    bufs.workspace, bufs.workspace_bytes = ws.data_ptr(), int(nbytes.value)
-
-    stream = torch.cuda.current_stream(dev)
-    run = lib.gdn_tm_run_f64 if f64 else lib.gdn_tm_run_f32
-    with torch.cuda.device(dev):
-        _native.check(run(ctypes.byref(params), ctypes.byref(pts), ctypes.byref(bufs),
-                          ctypes.c_void_p(stream.cuda_stream)))
-    # Keep host/device inputs alive until the stream has consumed them.
-    keep = (ws, ca, cb, eps, tabs, ik, src_cur, mx_cur, my_cur, port_vs, cb_src, cb_vs,
-            ph_e_t, ph_h_t, cw)
-    for t in _flatten(keep):
-        t.record_stream(stream)
-
-    return SimResult(
+    keep = (ca, cb, eps, tabs, ik, src_cur, mx_cur, my_cur, port_vs, cb_src, cb_vs, ph_e_t,
+            ph_h_t, cw)
+    host = (idx_arrays, cols, mon_arr)
+    result = SimResult(
         probe_ez=out_probe,
         energy=out_energy,
         ez=ez,
@@ -496,6 +465,78 @@ def simulate_tm(
         dft_hy=dft_out[2],
         monitors=mon_out if dft_monitors is not None else None,
     )
+    return _Prep(params, pts, bufs, keep, host, result, fdt == torch.float64, dev)
+
+
+def simulate_tm(
+    grid: Grid2D,
+    *,
+    source_ij=None,
+    source_current=None,
+    eps_r=1.0,
+    sigma=0.0,
+    probe_ij=(),
+    ports=(),
+    dft_freqs=(),
+    dft_dtype=None,
+    cpml: CPMLSpec = CPMLSpec(),
+    record_energy: bool = False,
+    mx_ij=None,
+    mx_current=None,
+    my_ij=None,
+    my_current=None,
+    dtype=None,
+    device=None,
+    dft_region=None,
+    dft_monitors=None,
+    cw_sources=None,
+) -> SimResult:
+    """Run a 2D TM FDTD simulation on the GPU (drop-in for fdtd2d.simulate_tm).
+
+    Arguments and semantics follow the reference (fdtd2d.py:181-247):
+    ``source_ij``/``source_current`` Jz line currents sampled at (n+1/2) dt;
+    ``eps_r``/``sigma`` scalars or (nx, ny); ``probe_ij`` Ez probes;
+    ``ports`` lumped RVS ports; ``dft_freqs`` running-DFT frequencies with
+    ``dft_dtype`` accumulators (default complex64 for float32 fields);
+    ``cpml``; ``record_energy``; ``mx_*``/``my_*`` magnetic currents on the
+    Hx/Hy grids injected as H -= (dt/mu) M.
+
+    Additions: ``dtype`` forces the field dtype; ``device`` selects the CUDA
+    device; ``dft_region`` = (ez_rect, hx_rect, hy_rect), each
+    (lo_i, lo_j, hi_i, hi_j) or None, limits the DFT to those rectangles;
+    ``dft_monitors`` = [(comp, lo_i, lo_j, hi_i, hi_j), ...] with comp 0/1/2 =
+    ez/hx/hy records only those boxes (returned in ``SimResult.monitors``,
+    dft_ez/hx/hy are then None); ``cw_sources`` = dict(env, src_w, mx_w, my_w) synthesises the Jz/Mx/My
+    waveforms on the device as env[n] Re(sum_k W_k exp(+i w_k t_n)) (the
+    frequency-domain adjoint's CW drive) instead of reading tabulated ones.
+    """
+    p = _prepare_tm(grid, source_ij=source_ij, source_current=source_current, eps_r=eps_r, sigma=sigma, probe_ij=probe_ij, ports=ports, dft_freqs=dft_freqs, dft_dtype=dft_dtype, cpml=cpml, record_energy=record_energy, mx_ij=mx_ij, mx_current=mx_current, my_ij=my_ij, my_current=my_current, dtype=dtype, device=device, dft_region=dft_region, dft_monitors=dft_monitors, cw_sources=cw_sources)
+    lib = _native.load()
+    nbytes = ctypes.c_size_t(0)
+    _native.check(lib.gdn_tm_workspace_size(ctypes.byref(p.params), ctypes.byref(p.pts),
+                                            int(p.f64), ctypes.byref(nbytes)))
+    ws = torch.empty(max(int(nbytes.value), 1), dtype=torch.uint8, device=p.dev)
+    p.bufs.workspace, p.bufs.workspace_bytes = ws.data_ptr(), int(nbytes.value)
+    stream = torch.cuda.current_stream(p.dev)
+    run = lib.gdn_tm_run_f64 if p.f64 else lib.gdn_tm_run_f32
+    with torch.cuda.device(p.dev):
+        _native.check(run(ctypes.byref(p.params), ctypes.byref(p.pts), ctypes.byref(p.bufs),
+                          ctypes.c_void_p(stream.cuda_stream)))
+    # Keep device inputs alive until the stream has consumed them.
+    for t in _flatten((ws, p.keep)):
+        t.record_stream(stream)
+    return p.result
+
+
+class _Prep(NamedTuple):
+    params: object
+    pts: object
+    bufs: object
+    keep: tuple
+    host: tuple
+    result: SimResult
+    f64: bool
+    dev: object
 
 
 def _flatten(x):

@@ -135,8 +135,9 @@ class _Plan(NamedTuple):
     objective_monitors: list | None
 
 
-def _forward(plan: _Plan, eps_r, sigma):
-    """Forward CW run: design-region Ez plus the objective's phasors."""
+def _forward_kwargs(plan: _Plan, eps_r, sigma):
+    """simulate_tm keyword arguments of the forward CW run: design-region Ez
+    plus the objective's phasors."""
     g = plan.grid
     (a0, a1), (b0, b1) = plan.bounds
     mons = [(0, a0, b0, a1, b1)]
@@ -144,11 +145,16 @@ def _forward(plan: _Plan, eps_r, sigma):
         mons += [(0, 0, 0, g.nx, g.ny), (1, 0, 0, g.nx, g.ny - 1), (2, 0, 0, g.nx - 1, g.ny)]
     else:
         mons += list(plan.objective_monitors)
-    res = simulate_tm(g, source_ij=plan.source_ij, source_current=plan.source_current,
-                      eps_r=eps_r, sigma=sigma, ports=plan.ports, dft_freqs=plan.freqs,
-                      dft_dtype=np.complex128, cpml=plan.cpml, dtype=plan.dtype,
-                      device=plan.device, dft_monitors=mons)
-    return res
+    return dict(grid=g, source_ij=plan.source_ij, source_current=plan.source_current,
+                eps_r=eps_r, sigma=sigma, ports=plan.ports, dft_freqs=plan.freqs,
+                dft_dtype=np.complex128, cpml=plan.cpml, dtype=plan.dtype, device=plan.device,
+                dft_monitors=mons)
+
+
+def _forward(plan: _Plan, eps_r, sigma):
+    """Forward CW run: design-region Ez plus the objective's phasors."""
+    kw = _forward_kwargs(plan, eps_r, sigma)
+    return simulate_tm(kw.pop("grid"), **kw)
 
 
 def _scatter_full(plan: _Plan, res):
@@ -202,16 +208,23 @@ def _adjoint_sources(plan: _Plan, cot):
     return out
 
 
-def _adjoint_run(plan: _Plan, eps_r, sigma, srcs):
+def _adjoint_kwargs(plan: _Plan, eps_r, sigma, srcs):
+    """simulate_tm keyword arguments of the adjoint run (None without sources)."""
     (a0, a1), (b0, b1) = plan.bounds
     (jz_idx, jz_w), (mx_idx, mx_w), (my_idx, my_w) = srcs
     if jz_idx is None and mx_idx is None and my_idx is None:
         return None
-    return simulate_tm(
-        plan.grid, source_ij=jz_idx, eps_r=eps_r, sigma=sigma, mx_ij=mx_idx, my_ij=my_idx,
-        dft_freqs=plan.freqs, dft_dtype=np.complex128, cpml=plan.cpml, dtype=plan.dtype,
-        device=plan.device, dft_monitors=[(0, a0, b0, a1, b1)],
-        cw_sources=dict(env=plan.env, src_w=jz_w, mx_w=mx_w, my_w=my_w))
+    return dict(grid=plan.grid, source_ij=jz_idx, eps_r=eps_r, sigma=sigma, mx_ij=mx_idx,
+                my_ij=my_idx, dft_freqs=plan.freqs, dft_dtype=np.complex128, cpml=plan.cpml,
+                dtype=plan.dtype, device=plan.device, dft_monitors=[(0, a0, b0, a1, b1)],
+                cw_sources=dict(env=plan.env, src_w=jz_w, mx_w=mx_w, my_w=my_w))
+
+
+def _adjoint_run(plan: _Plan, eps_r, sigma, srcs):
+    kw = _adjoint_kwargs(plan, eps_r, sigma, srcs)
+    if kw is None:
+        return None
+    return simulate_tm(kw.pop("grid"), **kw)
 
 
 def _contract(plan: _Plan, eps_r, sigma, e_d, lam_d, want_sigma, want_eps):

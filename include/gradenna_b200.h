@@ -175,6 +175,31 @@ int gdn_tm_run_f32(const GdnTmParams* p, const GdnTmPoints* pts,
 int gdn_tm_run_f64(const GdnTmParams* p, const GdnTmPoints* pts,
                    const GdnTmBuffers* b, void* stream);
 
+/* One problem of a batched run: the same three structs as gdn_tm_run_f32. */
+typedef struct GdnTmProblem {
+  const GdnTmParams* params;
+  const GdnTmPoints* points;
+  const GdnTmBuffers* buffers;
+} GdnTmProblem;
+
+/* Number of tile configurations a batched run can be forced to (cfg in
+ * [0, GDN_TM_NCFG)): 0 = 64x64 tiles, 4-step blocks; 1 = 32x64, 4;
+ * 2 = 16x32, 4; 3 = 64x64, 2; 4 = 32x64, 2 (float32 tile sizes). */
+#define GDN_TM_NCFG 5
+
+/* Run n independent float32 2D problems together (no reference counterpart:
+ * the reference runs one simulation per call). Every problem keeps its own
+ * grid, CPML, sources, ports, monitors and n_steps; each block of time
+ * steps is ONE launch per tile class over the tiles of all problems still
+ * running, so a population of small uneven grids fills the GPU. Results are
+ * identical to n separate gdn_tm_run_f32 calls with the same tile
+ * configuration. cfg = -1 picks the heuristic configuration of the largest
+ * problem; an autotuner passes the fastest measured one. Workspaces: a
+ * problem's buffers->workspace if given (gdn_tm_workspace_size bytes), else
+ * a stream-ordered block allocated for the call. record_energy is not
+ * supported in batched runs (GDN_ERR_BAD_ARG). */
+int gdn_tm_run_batch_f32(const GdnTmProblem* problems, int32_t n, int32_t cfg, void* stream);
+
 /* Allocation-free variant of gdn_tm_run_f32. No counterpart in the
  * reference: it exists for callers that must not allocate device memory
  * while they run the solver -- code that owns all GPU memory through its own
