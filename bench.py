@@ -95,10 +95,10 @@ def parse():
     ap.add_argument("--grid", type=int, default=N_GRID)
     ap.add_argument("--time-steps", type=int, default=None,
                     help="time steps per run (default: 8000 for tm2d, 6000 for patch3d)")
-    ap.add_argument("--workload", choices=("tm2d", "patch3d"), default="tm2d")
+    ap.add_argument("--workload", choices=("tm2d", "patch3d", "population"), default="tm2d")
     args = ap.parse_args()
     if args.time_steps is None:
-        args.time_steps = N_STEPS if args.workload == "tm2d" else P3_STEPS
+        args.time_steps = {"tm2d": N_STEPS, "patch3d": P3_STEPS, "population": 0}[args.workload]
     return args
 
 
@@ -189,6 +189,72 @@ def gradient_call3d(w, sigma_dev, vs_dev, dtype):
         port_resistance=RS, cpml=gb.CPMLSpec(P3_NPML), dtype=dtype,
         objective_kind=("port", "ntff_box"), box_margin=P3_BOX,
         eps_r_background=w["eps_bg"], sigma_background=w["sig_bg"])["sigma"]
+
+
+POP_N = 64
+
+
+def population(seed: int, n_problems: int = POP_N, max_steps: int = 0):
+    """64 seeded uneven 2D TM problems: square grids U{128..512} at 1 mm,
+    CPML U{10..16}, U{2000..6000} steps (capped by max_steps when > 0),
+    1-4 ports (the first driven by a CW sum of the problem's tones under a
+    300-step ramp, the others passive 50-ohm loads), 1-8 frequencies in
+    1-6 GHz, a seeded filtered/projected density on the central square of
+    half the side mapped by sigma_from_density, and the objective
+    sum_k P_rad,k (Poynting box 4 cells inside the CPML) - sum_k |S11_k|^2."""
+    import torch
+
+    import gradenna_b200 as gb
+    from gradenna_b200.materials import sigma_from_density
+    from gradenna_b200.monitors import poynting_box_monitors, port_monitors
+    from gradenna_b200.topopt import seeded_density
+
+    rng = np.random.default_rng(1000 + seed)
+    specs = []
+    for q in range(n_problems):
+        n = int(rng.integers(128, 513))
+        npml = int(rng.integers(10, 17))
+        steps = int(rng.integers(2000, 6001))
+        if max_steps > 0:
+            steps = min(steps, max_steps)
+        k = int(rng.integers(1, 9))
+        freqs = tuple(float(f) for f in np.sort(rng.uniform(1e9, 6e9, k)))
+        grid = gb.Grid2D(n, n, 1e-3, 1e-3)
+        d0, d1 = n // 4, n // 4 + n // 2
+        rho = seeded_density((n // 2, n // 2), seed=int(rng.integers(1 << 30)), radius_cells=3.0,
+                             beta=8.0, eta=0.5, device="cpu", dtype=torch.float64).numpy()
+        sig_d = np.asarray(sigma_from_density(rho), np.float64)
+        nn = np.arange(steps)
+        env = np.clip(nn / float(RAMP), 0.0, 1.0)
+        vs = env * sum(np.sin(2 * np.pi * f * (nn + 0.5) * grid.dt) for f in freqs)
+        lo, hi = npml + 3, d0 - 2
+        ports = []
+        for m in range(int(rng.integers(1, 5))):
+            ij = (int(rng.integers(lo, hi)), int(rng.integers(lo, n - lo)))
+            ports.append(gb.Port(ij, RS, vs if m == 0 else None))
+        b = npml + 4
+        box = (b, n - b - 1, b, n - b - 1)
+        mons = poynting_box_monitors(box)
+        for pt in ports:
+            mons += port_monitors(pt.ij)
+
+        def obj(ph, grid=grid, box=box):
+            from gradenna_b200.monitors import poynting_flux_box_2d
+            from gradenna_b200.sparams import s11_power_wave
+
+            pwr = poynting_flux_box_2d(ph.dft_ez, ph.dft_hx, ph.dft_hy, grid, box)
+            s = s11_power_wave(ph.port_v[:, 0], ph.port_i[:, 0], RS)
+            return pwr.sum() - (s.real**2 + s.imag**2).sum()
+
+        specs.append(dict(grid=grid, objective=obj, design_sigma=sig_d,
+                          design_region=(slice(d0, d1), slice(d0, d1)), dft_freqs=freqs, env=env,
+                          ports=tuple(ports), cpml=gb.CPMLSpec(npml), dtype=torch.float32,
+                          objective_monitors=mons))
+    return specs
+
+
+def pop_cells(specs):
+    return sum(sp["grid"].nx * sp["grid"].ny * len(sp["env"]) for sp in specs)
 
 
 def make_objective(grid, box):
@@ -366,8 +432,18 @@ def run_reference(args):
     world, rank, _ = dist_setup(args)
     if rank != 0:
         return 0
-    case = make_case(args, 0)
-    w = case["w"]
+    if args.workload == "population":
+        specs = population(0, max_steps=args.time_steps)
+        g0 = specs[0]["grid"]
+        case = dict(cells=pop_cells(specs) / (args.time_steps or 1),
+                    cpu=lambda dt: cpu_sample_pop(specs[0]),
+                    cpu_what=lambda n_s, t: (f"C oracle, forward + adjoint-shaped runs of {n_s} "
+                                             f"steps of population member 0 ({g0.nx}^2, {t:.1f} s)"),
+                    config={"workload": f"batched uneven population of {len(specs)} 2D TM "
+                                        "problems (see the GPU arm)",
+                            "problems": len(specs), "cell_steps_per_step": 2 * pop_cells(specs)})
+    else:
+        case = make_case(args, 0)
     dt_np = np.float32 if args.dtype == "f32" else np.float64
     vals = []
     n_s = None
@@ -376,12 +452,13 @@ def run_reference(args):
         if k >= args.warmup:
             vals.append(v)
     value = float(np.mean(vals))
-    cores = os.cpu_count() if args.workload == "tm2d" else 1
+    cores = os.cpu_count() if args.workload != "patch3d" else 1
     line = {
         "impl": "reference", "metric": "Gcell-steps/s fwd+adjoint", "value": value,
         "unit": "Gcell-steps/s", "n_gpus": args.gpus, "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": 2 * case["cells"] * args.time_steps / value / 1e6,
+        "ms_per_step": (2 * pop_cells(specs) if args.workload == "population"
+                        else 2 * case["cells"] * args.time_steps) / value / 1e6,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": args.dtype,
         "data": "synthetic",
         "config": case["config"],
@@ -470,6 +547,186 @@ def config3d(args, w):
         "design_cells": int(w["sigma_d"].size), "parallelism": f"replicas x{args.gpus}",
         "l2": "flushed (256 MiB write) before every timed step",
     }
+
+
+def _pop_forward_kwargs(specs, dev):
+    """simulate_tm keyword arguments of the forward runs of a population."""
+    from gradenna_b200 import freq_adjoint as fa
+
+    out = []
+    for sp in specs:
+        plan = fa._make_plan(sp["grid"], sp["design_region"], sp["dft_freqs"], sp["env"], None,
+                             None, sp["ports"], sp["cpml"], sp["dtype"], dev,
+                             sp["objective_monitors"])
+        eps_r, sigma = fa._full_eps_sigma(sp["grid"], sp["design_sigma"], None,
+                                          sp["design_region"], dev)
+        out.append(fa._forward_kwargs(plan, eps_r, sigma))
+    return out
+
+
+def cpu_sample_pop(spec, target_s: float = 10.0):
+    """C-oracle forward + adjoint-shaped runs of one population member for a
+    bounded number of steps (all host threads)."""
+    from oracle import fdtd2d_np as onp
+    from oracle.tm2d_c import simulate_tm_c
+
+    g = spec["grid"]
+    og = onp.Grid2D(g.nx, g.ny, g.dx, g.dy)
+    sigma = np.zeros((g.nx, g.ny))
+    sigma[spec["design_region"]] = np.asarray(spec["design_sigma"])
+    (a0, a1), (b0, b1) = [(r.start, r.stop) for r in spec["design_region"]]
+    mons = [(0, a0, b0, a1, b1)] + list(spec["objective_monitors"])
+
+    def run(n_s):
+        ports = tuple(onp.Port(p.ij, p.resistance,
+                               None if p.voltage is None else np.asarray(p.voltage)[:n_s])
+                      for p in spec["ports"])
+        kw = dict(sigma=sigma, ports=ports, dft_freqs=spec["dft_freqs"],
+                  cpml=onp.CPMLSpec(spec["cpml"].thickness), dtype=np.float32, dft_monitors=mons)
+        t0 = time.perf_counter()
+        simulate_tm_c(og, **kw)
+        simulate_tm_c(og, **kw)
+        return time.perf_counter() - t0
+
+    t = run(10)
+    n_s = int(np.clip(target_s / max(t, 1e-6) * 10, 20, len(spec["env"])))
+    t = run(n_s)
+    return 2 * g.nx * g.ny * n_s / t / 1e9, n_s, t
+
+
+def run_population(args):
+    """Batched forward + adjoint design gradients of a 64-member population."""
+    import torch
+
+    from gradenna_b200 import _native
+    from gradenna_b200.batch import autotune_tm_batch, freq_adjoint_gradient_batch
+    from gradenna_b200.freq_adjoint import freq_adjoint_gradient
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+        pg = dist
+    specs = population(rank, max_steps=args.time_steps)
+    dev_specs = [dict(sp, design_sigma=torch.as_tensor(sp["design_sigma"], device=dev))
+                 for sp in specs]
+    t0 = time.perf_counter()
+    best, tune = autotune_tm_batch(_pop_forward_kwargs(dev_specs, dev), probe_steps=64)
+    t_tune = time.perf_counter() - t0
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+
+    def call(sp):
+        return freq_adjoint_gradient_batch(sp, tile_config=best)
+
+    for _ in range(args.warmup):
+        call(dev_specs)
+    torch.cuda.synchronize()
+
+    def barrier():
+        if pg is not None:
+            pg.barrier()
+        torch.cuda.synchronize()
+
+    times = []
+    barrier()
+    l0 = _native.kernel_launches()
+    _native.tm_loop_stats(reset=True)
+    with ClockSampler(local) as clk:
+        for _ in range(args.steps):
+            flush.fill_(1.0)
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            g = call(dev_specs)
+            e1.record()
+            torch.cuda.synchronize()
+            times.append(e0.elapsed_time(e1) / 1e3)
+    launches = (_native.kernel_launches() - l0) // args.steps
+    loop_ms, loop_cells, _ = _native.tm_loop_stats(reset=True)
+    barrier()
+    t_step = float(np.mean(times))
+    assert all(torch.isfinite(x["sigma"]).all() for x in g)
+
+    # e2e: designs from pinned host memory, gradients read back.
+    hosts = [torch.as_tensor(sp["design_sigma"]).pin_memory() for sp in specs]
+    outs = [torch.empty(h.shape, dtype=torch.float64).pin_memory() for h in hosts]
+    e2e_times = []
+    for _ in range(args.steps):
+        flush.fill_(1.0)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        sp_e = [dict(sp, design_sigma=h.to(dev, non_blocking=True)) for sp, h in zip(specs, hosts)]
+        gg = call(sp_e)
+        for o, x in zip(outs, gg):
+            o.copy_(x["sigma"], non_blocking=True)
+        e1.record()
+        torch.cuda.synchronize()
+        e2e_times.append(e0.elapsed_time(e1) / 1e3)
+    t_e2e = float(np.mean(e2e_times))
+
+    # The same population one problem at a time (no batching), for reference.
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for sp in dev_specs:
+        sp = dict(sp)
+        freq_adjoint_gradient(sp.pop("grid"), sp.pop("objective"), **sp)
+    e1.record()
+    torch.cuda.synchronize()
+    t_single = e0.elapsed_time(e1) / 1e3
+
+    t_step, t_e2e = max_over_ranks(pg, [t_step, t_e2e], dev)
+    cell_steps = 2 * pop_cells(specs)
+    value = world * cell_steps / t_step / 1e9
+    e2e = world * cell_steps / t_e2e / 1e9
+    achieved = 8 * 4 * loop_cells / (loop_ms / 1e3) / 1e9
+    peak, peak_kind = measured_peak()
+    h2d = sum(h.numel() * h.element_size() for h in hosts)
+    cpu = None
+    if rank == 0:
+        v_cpu, n_s, t_cpu = cpu_sample_pop(specs[0])
+        cpu = {"value": v_cpu, "unit": "Gcell-steps/s", "cores": os.cpu_count(), "kind": "port",
+               "sample": f"C oracle, forward + adjoint-shaped runs of {n_s} steps of population "
+                         f"member 0 ({specs[0]['grid'].nx}^2, {t_cpu:.1f} s)"}
+        sides = [sp["grid"].nx for sp in specs]
+        line = {
+            "metric": "Gcell-steps/s fwd+adjoint", "value": value, "unit": "Gcell-steps/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": {
+                "workload": f"batched uneven population: {len(specs)} 2D TM problems, square "
+                            f"grids {min(sides)}-{max(sides)} at 1 mm, CPML 10-16, 2000-6000 "
+                            "steps, 1-4 ports, 1-8 DFT frequencies in 1-6 GHz, seeded "
+                            "filtered/projected designs; freq-adjoint gradient of each",
+                "problems": len(specs), "cell_steps_per_step": cell_steps,
+                "autotuned_tile_config": best,
+                "autotune_s": t_tune, "autotune_probe_s": {str(k): v for k, v in tune.items()},
+                "unbatched_ms": t_single * 1e3,
+                "unbatched_value": cell_steps / t_single / 1e9,
+                "parallelism": f"replicas x{world}",
+                "l2": "flushed (256 MiB write) before every timed step"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "kernel": "tm_tb_batch block launches of both passes (time loops incl. "
+                                   "DFT folds; 32 B per cell-step)",
+                         "peak_source": peak_kind,
+                         "loop_share_of_step": loop_ms / 1e3 / (t_step * args.steps)},
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e, "unit": "Gcell-steps/s", "h2d_bytes_per_step": int(h2d),
+                    "d2h_bytes_per_step": int(h2d)},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
 
 
 def run_ours(args):
@@ -597,6 +854,8 @@ def main():
     args = parse()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload == "population":
+        return run_population(args)
     return run_ours(args)
 
 
