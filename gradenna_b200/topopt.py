@@ -1,6 +1,7 @@
-"""Design-parameterisation pieces used to build design densities
-(src/gradenna/topopt.py:55-150): conic filter, tanh projection, the
-sigmoid -> filter -> projection transform and the beta continuation.
+"""Topology-optimisation pieces (src/gradenna/topopt.py): conic filter,
+tanh projection, the sigmoid -> filter -> projection transform, beta
+continuation, the gray indicator, the fabrication checks and the Adam
+driver ``optimize``.
 
 torch implementations (differentiable, any device). The conic filter is a
 direct "same" convolution with the renormalised boundary of the reference
@@ -28,16 +29,18 @@ def conic_kernel(radius_cells: float, ndim: int = 2) -> np.ndarray:
 
 
 def conic_filter(rho: torch.Tensor, radius_cells: float) -> torch.Tensor:
-    """(K * rho) / (K * 1) with a conic kernel of radius R cells (topopt.py:65-90)."""
+    """(K * rho) / (K * 1) with a conic kernel of radius R cells, for 1D, 2D
+    or 3D densities (topopt.py:65-90)."""
     radius = float(radius_cells)
     if radius <= 1.0:
         return rho
-    if rho.ndim != 2:
-        raise ValueError("conic_filter here supports 2D densities")
-    k = torch.as_tensor(conic_kernel(radius, 2), dtype=rho.dtype, device=rho.device)
+    if rho.ndim not in (1, 2, 3):
+        raise ValueError("conic_filter supports 1D, 2D and 3D densities")
+    conv = {1: F.conv1d, 2: F.conv2d, 3: F.conv3d}[rho.ndim]
+    k = torch.as_tensor(conic_kernel(radius, rho.ndim), dtype=rho.dtype, device=rho.device)
     pad = k.shape[0] // 2
-    num = F.conv2d(rho[None, None], k[None, None], padding=pad)[0, 0]
-    den = F.conv2d(torch.ones_like(rho)[None, None], k[None, None], padding=pad)[0, 0]
+    num = conv(rho[None, None], k[None, None], padding=pad)[0, 0]
+    den = conv(torch.ones_like(rho)[None, None], k[None, None], padding=pad)[0, 0]
     return num / den
 
 
@@ -83,3 +86,99 @@ def seeded_density(shape, seed: int = 0, radius_cells: float = 3.0, beta: float 
     noise = np.random.default_rng(seed).uniform(0.0, 1.0, size=shape)
     rho = torch.as_tensor(noise, dtype=dtype, device=device)
     return tanh_projection(conic_filter(rho, radius_cells), beta, eta)
+
+
+def gray_indicator(rho: torch.Tensor) -> torch.Tensor:
+    """Mean of 4 rho (1 - rho): 0 for a binary field, 1 at rho = 0.5 (topopt.py:153-155)."""
+    return torch.mean(4.0 * rho * (1.0 - rho))
+
+
+# ---------------------------------------------------------------------------
+# Post-processing checks (host, non-differentiable; topopt.py:158-237)
+# ---------------------------------------------------------------------------
+
+
+def _np(x):
+    return x.detach().cpu().numpy() if isinstance(x, torch.Tensor) else np.asarray(x)
+
+
+def connected_to_seed(rho_binary, seed_ij) -> np.ndarray:
+    """Solid (> 0.5) 4-connected component containing the seed pixel; all
+    False when the seed is not solid (topopt.py:163-184)."""
+    from scipy import ndimage
+
+    solid = _np(rho_binary) > 0.5
+    labels, _ = ndimage.label(solid)
+    lab = labels[tuple(int(v) for v in seed_ij)]
+    if lab == 0:
+        return np.zeros_like(solid, dtype=bool)
+    return labels == lab
+
+
+def _disk_footprint(width_cells: int) -> np.ndarray:
+    """Disk of radius (w - 1) / 2 cells (topopt.py:187-199)."""
+    radius = (width_cells - 1) / 2.0
+    n = int(np.floor(radius))
+    y, x = np.mgrid[-n:n + 1, -n:n + 1]
+    return (x * x + y * y) <= radius * radius + 1e-9
+
+
+def minimum_feature_size(rho_binary, width_cells: int) -> np.ndarray:
+    """Solid pixels removed by a binary opening with the disk footprint: the
+    features thinner than the minimum width (topopt.py:202-237). Erosion
+    treats the domain edge as solid, so clipped features are not flagged."""
+    from scipy import ndimage
+
+    solid = _np(rho_binary) > 0.5
+    if width_cells <= 1:
+        return np.zeros_like(solid, dtype=bool)
+    fp = _disk_footprint(int(width_cells))
+    eroded = ndimage.binary_erosion(solid, structure=fp, border_value=1)
+    opened = ndimage.binary_dilation(eroded, structure=fp, border_value=0)
+    return solid & ~opened
+
+
+# ---------------------------------------------------------------------------
+# Optimisation driver (topopt.py:245-319)
+# ---------------------------------------------------------------------------
+
+
+def optimize(loss_fn, theta0, n_steps: int = 400, betas=(8.0, 16.0, 32.0, 64.0),
+             learning_rate: float = 0.02, transform: DesignTransform | None = None,
+             n_snapshots: int = 4) -> dict:
+    """Adam with beta continuation over the three-field parameterisation.
+
+    ``loss_fn(rho, beta)`` returns a scalar tensor differentiable in rho by
+    torch autograd (for FDTD objectives: freq_adjoint_objective, whose
+    backward is the two-run adjoint on the GPU). ``theta0`` is the latent
+    design; it stays on its device, where the transform and the Adam update
+    (torch.optim.Adam: beta1 0.9, beta2 0.999, eps 1e-8, the optax.adam
+    defaults of the reference) run. ``n_steps`` are split evenly over
+    ``betas``. Returns the reference's dict: "theta", "rho" (the final theta
+    projected at the final beta), per-step "loss", "gray" and "beta" arrays,
+    and "snapshots" [(step, rho numpy)].
+    """
+    if transform is None:
+        transform = DesignTransform(radius_cells=2.0)
+    betas = tuple(betas)
+    schedule = beta_schedule(betas, max(1, n_steps // len(betas)))
+    theta = torch.as_tensor(theta0).detach().clone().requires_grad_(True)
+    opt = torch.optim.Adam([theta], lr=learning_rate, betas=(0.9, 0.999), eps=1e-8)
+    snap_at = set(int(round(v)) for v in np.linspace(0, n_steps - 1, max(1, n_snapshots)))
+    losses, grays, beta_hist, snaps = [], [], [], []
+    for i in range(n_steps):
+        beta = schedule(i)
+        opt.zero_grad(set_to_none=True)
+        rho = transform(theta, beta)
+        loss = loss_fn(rho, beta)
+        loss.backward()
+        opt.step()
+        losses.append(float(loss.detach()))
+        grays.append(float(gray_indicator(rho.detach())))
+        beta_hist.append(beta)
+        if i in snap_at:
+            snaps.append((i, rho.detach().cpu().numpy()))
+    with torch.no_grad():
+        rho = transform(theta, schedule(max(0, n_steps - 1)))
+    return {"theta": theta.detach(), "rho": rho, "loss": np.asarray(losses),
+            "gray": np.asarray(grays), "beta": np.asarray(beta_hist), "snapshots": snaps}
