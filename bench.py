@@ -398,7 +398,7 @@ def profiled_traffic(name):
     try:
         for line in open(path):
             if line.startswith("traffic_bytes_per_launch:"):
-                return int(float(line.split(":", 1)[1]))
+                return int(float(line.split(":", 1)[1].split()[0]))
     except OSError:
         pass
     return None

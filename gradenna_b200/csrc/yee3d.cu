@@ -82,6 +82,8 @@ struct Dev3 {
   const Mon3* mons;
   const int* mw_off;  // per-CTA CSR over mw
   const MonW3* mw;
+  T* cwv;                // CW source values of the chunk: [sub][cw_off[type] + m]
+  long long cw_total, cw_off[6];
   const int* step_base;
 };
 
@@ -93,17 +95,40 @@ __device__ __forceinline__ long long at(const Dev3<T>& d, int i, int j, int k) {
   return ((long long)(i + 1) * d.sy + (j + 1)) * d.sz + (k + 1);
 }
 
+// Source value of point m of channel `type` at step n (chunk offset sub):
+// tabulated, or the chunk's CW values synthesised by yee_cw_synth.
 template <typename T>
-__device__ __forceinline__ T wave(const Dev3<T>& d, int type, int n_pts, int m, int n) {
-  if (!d.cw) return d.cur[type][(long long)n * n_pts + m];
-  double s = 0.0;
+__device__ __forceinline__ T wave(const Dev3<T>& d, int type, int n_pts, int m, int n, int sub) {
+  if (d.cw) return d.cwv[(long long)sub * d.cw_total + d.cw_off[type] + m];
+  return d.cur[type][(long long)n * n_pts + m];
+}
+
+// CW source values J(n) = env[n] Re(sum_k W_k conj(ph[n,k])) of every point
+// for the `cnt` steps of a chunk, once per chunk instead of once per step.
+template <typename T>
+__global__ void yee_cw_synth(Dev3<T> d, int cnt) {
+  const long long mg = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (mg >= d.cw_total) return;
+  int type = 0;
+#pragma unroll
+  for (int t = 1; t < 6; ++t)
+    if (mg >= d.cw_off[t]) type = t;
+  const long long m = mg - d.cw_off[type];
+  const double2* w = d.w[0];
+#pragma unroll
+  for (int t = 1; t < 6; ++t)
+    if (type == t) w = d.w[t];
   const double2* ph = type <= 2 ? d.ph_e : d.ph_h;
-  for (int k = 0; k < d.n_freq; ++k) {
-    const double2 a = d.w[type][(long long)m * d.n_freq + k];
-    const double2 p = ph[(long long)n * d.n_freq + k];
-    s += a.x * p.x + a.y * p.y;
+  const int n0 = *d.step_base, K = d.n_freq;
+  for (int t = 0; t < cnt; ++t) {
+    double s = 0.0;
+    for (int k = 0; k < K; ++k) {
+      const double2 a = w[m * K + k];
+      const double2 p = ph[(long long)(n0 + t) * K + k];
+      s += a.x * p.x + a.y * p.y;
+    }
+    d.cwv[(long long)t * d.cw_total + mg] = T(d.cw_env[n0 + t] * s);
   }
-  return T(d.cw_env[n] * s);
 }
 
 // CPML term of one derivative along axis `ax` at sample index `s` of that
@@ -196,7 +221,7 @@ __global__ void __launch_bounds__(NT) yee_h(Dev3<T> d, int sub) {
       const int np_ = t == 3 ? d.n_mx : (t == 4 ? d.n_my : d.n_mz);
       for (int q = d.off[t][cta] + tid; q < d.off[t][cta + 1]; q += NT) {
         const Pt3 p = d.pts[t][q];
-        atomicAdd(hs[t - 3] + at(d, p.i, p.j, p.k), -(d.dt_mu * wave(d, t, np_, p.m, n)));
+        atomicAdd(hs[t - 3] + at(d, p.i, p.j, p.k), -(d.dt_mu * wave(d, t, np_, p.m, n, sub)));
       }
     }
   }
@@ -268,7 +293,7 @@ __global__ void __launch_bounds__(NT) yee_e(Dev3<T> d, int sub) {
     for (int t = 0; t < 3; ++t)
       for (int q = d.off[t][cta] + tid; q < d.off[t][cta + 1]; q += NT) {
         const Pt3 p = d.pts[t][q];
-        atomicAdd(es[t] + at(d, p.i, p.j, p.k), -(cbs[t][p.m] * wave(d, t, nps[t], p.m, n)));
+        atomicAdd(es[t] + at(d, p.i, p.j, p.k), -(cbs[t][p.m] * wave(d, t, nps[t], p.m, n, sub)));
       }
     __syncthreads();
     if (port_here && tid == 0) {
@@ -466,7 +491,7 @@ static void comp_shape(int c, int nx, int ny, int nz, int s[3]) {
 struct Layout3 {
   int sy = 0, sz = 0, gj = 0, gk = 0, n_cta = 0, R = 32;
   long long vol = 0, mon_cells = 0, n_mw = 0;
-  size_t fields, psi, zero_end, off[7], pts[7], mons, mw_off, mw, mring, step, eacc, total;
+  size_t fields, psi, zero_end, off[7], pts[7], mons, mw_off, mw, mring, step, eacc, cwv, total;
 };
 
 // Monitor boxes {comp, lo0, lo1, lo2, s0, s1, s2} in ring order: the listed
@@ -555,6 +580,10 @@ static Layout3 make_layout3(const GdnYeeParams* p, const GdnYeePoints* pts, size
   L.mw = cv.take<MonW3>(size_t(std::max<long long>(L.n_mw, 1)));
   L.mring = cv.take<char>(std::max<size_t>(size_t(L.mon_cells) * L.R, 1) * esize);
   L.eacc = cv.take<double>(p->record_energy ? 2 * size_t(std::max(p->n_steps, 1)) : 1);
+  long long cw_total = 0;
+  if (p->cw_sources)
+    for (int t = 0; t < 6; ++t) cw_total += count_of(p, t);
+  L.cwv = cv.take<char>(size_t(std::max<long long>(cw_total * L.R, 1)) * esize);
   L.total = cv.bytes();
   return L;
 }
@@ -726,6 +755,12 @@ static int run3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuff
   d.mon_cells = L.mon_cells;
   int* step_base = reinterpret_cast<int*>(ws + L.step);
   d.step_base = step_base;
+  d.cwv = reinterpret_cast<T*>(ws + L.cwv);
+  d.cw_total = 0;
+  for (int t = 0; t < 6; ++t) {
+    d.cw_off[t] = d.cw_total;
+    if (p->cw_sources) d.cw_total += count_of(p, t);
+  }
 
   // Point bins by CTA box (i, j/BJ, k/BK).
   for (int t = 0; t < 7; ++t) {
@@ -826,6 +861,10 @@ static int run3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuff
   const int eblocks = int(std::min<long long>(div_up((long long)nx * ny * nz, 256), 148 * 8));
   auto enqueue = [&](int cnt, cudaStream_t s) -> uint64_t {
     uint64_t k = 0;
+    if (d.cw_total > 0) {
+      yee_cw_synth<T><<<unsigned(div_up(d.cw_total, 256)), 256, 0, s>>>(d, cnt);
+      ++k;
+    }
     for (int t = 0; t < cnt; ++t) {
       yee_h<T><<<grd, blk, 0, s>>>(d, t);
       yee_e<T><<<grd, blk, 0, s>>>(d, t);
