@@ -171,7 +171,7 @@ def freq_adjoint_gradient_batch(specs, *, tile_config: int | None = None, device
         plan = fa._make_plan(grid, sp["design_region"], sp["dft_freqs"], sp["env"],
                              sp.get("source_ij"), sp.get("source_current"), sp.get("ports", ()),
                              sp.get("cpml", fa.CPMLSpec()), sp.get("dtype", torch.float32), dev,
-                             sp.get("objective_monitors"))
+                             sp.get("objective_monitors"), sp.get("exact", True))
         if plan.dtype != torch.float32:
             raise ValueError("batched gradients are float32")
         eps_r, sigma = fa._full_eps_sigma(grid, ds, de, sp["design_region"], dev)

@@ -137,7 +137,7 @@ __global__ void poynting_grad_kernel(Box b, double dx, double dy, const C* ez, c
 __global__ void contract_kernel(int n_cells, int K, double dt, double k_norm,
                                 const double2* e_fwd, const double2* lam, const double* eps_r,
                                 const double* sigma, const double2* z, double* g_sig,
-                                double* g_eps) {
+                                double* g_eps, int flags) {
   const int c = blockIdx.x * blockDim.x + threadIdx.x;
   if (c >= n_cells) return;
   const double EPS0 = 1.0 / (1.25663706212e-06 * 299792458.0 * 299792458.0);
@@ -166,8 +166,14 @@ __global__ void contract_kernel(int n_cells, int K, double dt, double k_norm,
     gs += k_norm * (l.x * g1.x - l.y * g1.y);
     ge += k_norm * (l.x * g2.x - l.y * g2.y);
   }
-  if (g_sig) g_sig[c] = er * gs;
-  if (g_eps) g_eps[c] = er * ge;
+  // The adjoint Ez phasor is recorded on the vacuum source basis; the cell's
+  // own update uses c_b = (dt / eps) / (1 + h), so the adjoint amplitude
+  // carries 1 / (eps_r (1 + h)) relative to vacuum. The reference undoes
+  // only the eps_r part (freq_adjoint.py:474-486), which is exact for
+  // h << 1 only; GDN_CONTRACT_EXACT_LOSS undoes both.
+  const double scale = (flags & GDN_CONTRACT_EXACT_LOSS) ? er * (1.0 + h) : er;
+  if (g_sig) g_sig[c] = scale * gs;
+  if (g_eps) g_eps[c] = scale * ge;
 }
 
 static int check_box(int nx, int ny, int n_freq, const int32_t* box) {
@@ -238,7 +244,7 @@ extern "C" int gdn_poynting_box_2d_grad(int32_t nx, int32_t ny, int32_t n_freq,
 extern "C" int gdn_tm_adjoint_contract(int32_t n_cells, int32_t n_freq, double dt, double k_norm,
                                        const void* e_fwd, const void* lam, const double* eps_r,
                                        const double* sigma, const void* z, double* grad_sigma,
-                                       double* grad_eps_r, void* stream) {
+                                       double* grad_eps_r, int32_t flags, void* stream) {
   if (n_cells < 0 || n_freq < 0) GDN_BAD_ARG("negative size");
   if (n_cells == 0) return GDN_OK;
   if (!e_fwd || !lam || !eps_r || !sigma || !z) GDN_BAD_ARG("null input pointer");
@@ -247,7 +253,7 @@ extern "C" int gdn_tm_adjoint_contract(int32_t n_cells, int32_t n_freq, double d
                     static_cast<cudaStream_t>(stream)>>>(
       n_cells, n_freq, dt, k_norm, static_cast<const double2*>(e_fwd),
       static_cast<const double2*>(lam), eps_r, sigma, static_cast<const double2*>(z), grad_sigma,
-      grad_eps_r);
+      grad_eps_r, flags);
   gdn::count_launches(1);
   GDN_TRY_CUDA(cudaGetLastError());
   return GDN_OK;

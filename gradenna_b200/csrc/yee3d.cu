@@ -237,7 +237,7 @@ __global__ void __launch_bounds__(NT) yee_h(Dev3<T> d, int sub) {
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(NT) yee_e(Dev3<T> d, int sub) {
-  __shared__ T s_port[2];  // Ez^n and curl_z at the port edge
+  __shared__ T s_port[3];  // Ez^n, curl_z and the plain-updated Ez at the port edge
   const int n = *d.step_base + sub;
   const int k = blockIdx.x * BK + threadIdx.x;
   const int j = blockIdx.y * BJ + threadIdx.y;
@@ -274,11 +274,13 @@ __global__ void __launch_bounds__(NT) yee_e(Dev3<T> d, int sub) {
       const T tx = cpml<T, true>(d, 0, i - 1, nx - 2, dhy_dx, d.psi + P_EZX * d.vol + c);
       const T ty = cpml<T, true>(d, 1, j - 1, ny - 2, dhx_dy, d.psi + P_EZY * d.vol + c);
       const T curl = tx - ty;
+      const T upd = d.ca[g] * ez[c] + d.cb[g] * curl;
       if (port_here && i == d.pi && j == d.pj && k == d.pk) {
         s_port[0] = ez[c];
         s_port[1] = curl;
+        s_port[2] = upd;
       }
-      ez[c] = d.ca[g] * ez[c] + d.cb[g] * curl;
+      ez[c] = upd;
     }
   }
   const int tid = threadIdx.y * BK + threadIdx.x;
@@ -298,7 +300,12 @@ __global__ void __launch_bounds__(NT) yee_e(Dev3<T> d, int sub) {
     __syncthreads();
     if (port_here && tid == 0) {
       const long long c = at(d, d.pi, d.pj, d.pk);
-      const T ez_new = d.a_port * s_port[0] + d.b_port * s_port[1] + d.c_port * d.port_vs[n];
+      // A current source on the port edge enters the port's semi-implicit
+      // update like the curl does: its plain increment (ez - upd, added by
+      // the source loop above) rescaled from c_b to the port's b.
+      const T src = ez[c] - s_port[2];
+      const T ez_new = d.a_port * s_port[0] + d.b_port * s_port[1] + d.c_port * d.port_vs[n] +
+                       (src != T(0) ? src * (d.b_port / d.cb[((long long)d.pi * ny + d.pj) * nz + d.pk]) : T(0));
       ez[c] = ez_new;
       d.out_v[n] = T(-0.5) * d.dz * (s_port[0] + ez_new);
       const long long dj = d.sz, di = (long long)d.sy * d.sz;

@@ -50,7 +50,10 @@ Q_MAG = -EPS0 / MU0
 _native.register("gdn_tm_adjoint_contract", ctypes.c_int, [
     ctypes.c_int32, ctypes.c_int32, ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
     ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p,
-    ctypes.c_void_p, ctypes.c_void_p])
+    ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p])
+
+#: gdn_tm_adjoint_contract flag: scale by eps_r (1 + h) instead of eps_r.
+CONTRACT_EXACT_LOSS = 1
 
 
 class FreqPhasors(NamedTuple):
@@ -133,6 +136,7 @@ class _Plan(NamedTuple):
     dtype: torch.dtype
     device: torch.device
     objective_monitors: list | None
+    exact: bool = True
 
 
 def _forward_kwargs(plan: _Plan, eps_r, sigma):
@@ -214,9 +218,14 @@ def _adjoint_kwargs(plan: _Plan, eps_r, sigma, srcs):
     (jz_idx, jz_w), (mx_idx, mx_w), (my_idx, my_w) = srcs
     if jz_idx is None and mx_idx is None and my_idx is None:
         return None
+    # The reference's adjoint run has no ports (freq_adjoint.py:437-450). A
+    # lumped port is a resistor in the medium, so the exact adjoint keeps it
+    # as a passive load (no source voltage).
+    ports = tuple(Port(p.ij, p.resistance, None) for p in plan.ports) if plan.exact else ()
     return dict(grid=plan.grid, source_ij=jz_idx, eps_r=eps_r, sigma=sigma, mx_ij=mx_idx,
-                my_ij=my_idx, dft_freqs=plan.freqs, dft_dtype=np.complex128, cpml=plan.cpml,
-                dtype=plan.dtype, device=plan.device, dft_monitors=[(0, a0, b0, a1, b1)],
+                my_ij=my_idx, ports=ports, dft_freqs=plan.freqs, dft_dtype=np.complex128,
+                cpml=plan.cpml, dtype=plan.dtype, device=plan.device,
+                dft_monitors=[(0, a0, b0, a1, b1)],
                 cw_sources=dict(env=plan.env, src_w=jz_w, mx_w=mx_w, my_w=my_w))
 
 
@@ -248,26 +257,28 @@ def _contract(plan: _Plan, eps_r, sigma, e_d, lam_d, want_sigma, want_eps):
     with torch.cuda.device(plan.device):
         _native.check(lib.gdn_tm_adjoint_contract(
             n_cells, K, dt, k_norm, e.data_ptr(), lam.data_ptr(), er.data_ptr(), sg.data_ptr(),
-            z.data_ptr(), _native.ptr(gs), _native.ptr(ge), stream))
+            z.data_ptr(), _native.ptr(gs), _native.ptr(ge),
+            CONTRACT_EXACT_LOSS if plan.exact else 0, stream))
     shape = e_d.shape[1:]
     return (None if gs is None else gs.reshape(shape)), (None if ge is None else ge.reshape(shape))
 
 
 def _make_plan(grid, design_region, dft_freqs, env, source_ij, source_current, ports, cpml,
-               dtype, device, objective_monitors):
+               dtype, device, objective_monitors, exact=True):
     dev = _native.require_cuda(device)
     freqs = tuple(float(f) for f in dft_freqs)
     env = np.asarray(env.detach().cpu() if isinstance(env, torch.Tensor) else env, np.float64)
     bounds = _region_bounds(design_region, grid.shape)
     ports = tuple(p if isinstance(p, Port) else Port(*p) for p in ports)
     return _Plan(grid, freqs, env, tuple(design_region), bounds, source_ij, source_current, ports,
-                 cpml, dtype, dev, objective_monitors)
+                 cpml, dtype, dev, objective_monitors, bool(exact))
 
 
 def freq_adjoint_gradient(grid: Grid2D, objective, *, design_sigma=None, design_eps_r=None,
                           design_region, dft_freqs, env, source_ij=None, source_current=None,
                           ports=(), cpml: CPMLSpec = CPMLSpec(), backend: str = "cuda",
-                          dtype=torch.float64, device=None, objective_monitors=None):
+                          dtype=torch.float64, device=None, objective_monitors=None,
+                          exact: bool = True):
     """Two-run frequency-domain adjoint gradient (freq_adjoint.py:355-493).
 
     ``objective`` maps FreqPhasors (torch complex128 on the device) to a real
@@ -281,11 +292,17 @@ def freq_adjoint_gradient(grid: Grid2D, objective, *, design_sigma=None, design_
     the reference's 3D DFTRegions); other phasors are then zero and the
     forward run records far less DFT data. ``dtype`` is the field dtype of
     both runs (float64 like the reference's freq-adjoint solves).
+    ``exact`` (default) keeps the ports in the adjoint run as passive
+    resistive loads and scales the contraction by eps_r (1 + sigma dt /
+    (2 eps)), which makes the gradient match the exact time-domain gradient
+    for port-driven and lossy designs; ``exact=False`` reproduces the
+    reference's formulas (port-less adjoint run, eps_r scaling), which agree
+    only for small sigma and no ports.
     """
     if backend not in ("xla", "native", "cuda"):
         raise ValueError(f"backend must be 'xla', 'native' or 'cuda', got {backend!r}")
     plan = _make_plan(grid, design_region, dft_freqs, env, source_ij, source_current, ports,
-                      cpml, dtype, device, objective_monitors)
+                      cpml, dtype, device, objective_monitors, exact)
     eps_r, sigma = _full_eps_sigma(grid, design_sigma, design_eps_r, design_region, plan.device)
     fwd = _forward(plan, eps_r, sigma)
     full = _scatter_full(plan, fwd)
@@ -341,10 +358,10 @@ class FreqAdjointObjective(torch.autograd.Function):
 def freq_adjoint_objective(design_sigma, grid: Grid2D, objective, *, design_region, dft_freqs,
                            env, source_ij=None, source_current=None, ports=(),
                            cpml: CPMLSpec = CPMLSpec(), dtype=torch.float64, device=None,
-                           objective_monitors=None):
+                           objective_monitors=None, exact: bool = True):
     """Differentiable objective value: ``.backward()`` runs the adjoint."""
     plan = _make_plan(grid, design_region, dft_freqs, env, source_ij, source_current, ports,
-                      cpml, dtype, device, objective_monitors)
+                      cpml, dtype, device, objective_monitors, exact)
     return FreqAdjointObjective.apply(design_sigma, plan, objective)
 
 

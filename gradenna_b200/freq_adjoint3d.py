@@ -154,8 +154,9 @@ def _adjoint_channels(grid, cot):
     return out
 
 
-def _contract(grid, freqs, env, eps_d, sig_d, e_fwd, lam, want_sigma, want_eps):
-    """Per-cell gradient of one E component (gdn_tm_adjoint_contract)."""
+def _contract(grid, freqs, env, eps_d, sig_d, e_fwd, lam, want_sigma, want_eps, exact=True):
+    """Per-cell gradient of one E component (gdn_tm_adjoint_contract; with
+    ``exact`` the contraction carries the loss factor 1 + sigma dt / (2 eps))."""
     dt = grid.dt
     K = len(freqs)
     n_eff = float(np.sum(np.asarray(env, np.float64) ** 2))
@@ -172,7 +173,8 @@ def _contract(grid, freqs, env, eps_d, sig_d, e_fwd, lam, want_sigma, want_eps):
     with torch.cuda.device(e.device):
         _native.check(_native.load().gdn_tm_adjoint_contract(
             n, K, dt, 2.0 / (n_eff * dt), e.data_ptr(), lm.data_ptr(), er.data_ptr(),
-            sg.data_ptr(), z.data_ptr(), _native.ptr(gs), _native.ptr(ge), stream))
+            sg.data_ptr(), z.data_ptr(), _native.ptr(gs), _native.ptr(ge),
+            1 if exact else 0, stream))
     return gs, ge
 
 
@@ -182,7 +184,7 @@ def freq_adjoint_gradient_3d(grid: Grid3D, objective, *, design_sigma=None, desi
                              cpml: CPMLSpec = CPMLSpec(), backend: str = "cuda",
                              objective_kind: str | None = None, box_margin: int | None = None,
                              monitor_region=None, dtype=torch.float64, device=None,
-                             eps_r_background=None, sigma_background=None):
+                             eps_r_background=None, sigma_background=None, exact: bool = True):
     """Two-run 3D frequency-domain adjoint gradient (freq_adjoint.py:864-1065).
 
     ``objective`` maps FreqPhasors3D (torch complex128 on the device) to a
@@ -197,7 +199,11 @@ def freq_adjoint_gradient_3d(grid: Grid3D, objective, *, design_sigma=None, desi
     reads). ``eps_r_background`` / ``sigma_background`` (nx, ny, nz)
     replace the reference's vacuum background (an addition: fixed structures
     such as a substrate and ground plane around the design); the design
-    values overwrite them on design_region. ``backend`` is accepted for signature compatibility
+    values overwrite them on design_region. ``exact`` (default) keeps the
+    port in the adjoint run as a passive load and scales the contraction by
+    eps_r (1 + sigma dt / (2 eps)); ``exact=False`` reproduces the
+    reference's formulas, which hold only for small sigma and no port.
+    ``backend`` is accepted for signature compatibility
     ("xla", "native", "cuda"); every run is the CUDA path. Returns
     {"sigma": ..., "eps_r": ...} (float64 tensors of the design shape) for
     the design variables supplied.
@@ -280,6 +286,11 @@ def freq_adjoint_gradient_3d(grid: Grid3D, objective, *, design_sigma=None, desi
     for key, (idx, w) in chans.items():
         kw[names[key][0]] = idx
         cw[f"{key}_w"] = w
+    if exact and pijk is not None:
+        # The lumped port is a resistor in the medium: the exact adjoint run
+        # keeps it as a passive load (the reference's adjoint run drops it).
+        kw.update(port_ijk=pijk, port_resistance=port_resistance,
+                  port_voltage=np.zeros(len(np.asarray(env)), np.float64))
     adj = simulate_3d(grid, dft_monitors=adj_boxes, cw_sources=cw, **kw, **common)
     ad = phasors(adj, adj_boxes)
 
@@ -288,7 +299,7 @@ def freq_adjoint_gradient_3d(grid: Grid3D, objective, *, design_sigma=None, desi
     gs_tot = ge_tot = None
     for e_full, l_full in ((fd.ex, ad.ex), (fd.ey, ad.ey), (fd.ez, ad.ez)):
         gs, ge = _contract(grid, freqs, env, eps_d, sig_d, e_full[sel], l_full[sel],
-                           design_sigma is not None, design_eps_r is not None)
+                           design_sigma is not None, design_eps_r is not None, exact)
         if gs is not None:
             gs_tot = gs if gs_tot is None else gs_tot + gs
         if ge is not None:

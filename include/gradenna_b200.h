@@ -310,16 +310,19 @@ int gdn_poynting_box_2d_grad(int32_t nx, int32_t ny, int32_t n_freq, const int32
 
 /* Design-cell gradient of the frequency-domain adjoint (replaces the numpy
  * contraction of freq_adjoint_gradient, src/gradenna/freq_adjoint.py:454-493):
- *   dL/dtheta = eps_r * sum_k k_norm Re[conj(lam_k) conj(G_k)],
+ *   dL/dtheta = s * sum_k k_norm Re[conj(lam_k) conj(G_k)],
  *   G_k = dca E_k / z_k + dcb (E_k - ca E_k / z_k) / cb,  z_k = exp(i w_k dt),
- * with the closed-form dca, dcb of freq_adjoint.py:186-206. All arrays are
- * DEVICE: e_fwd, lam (n_freq, n_cells) complex128; eps_r, sigma (n_cells)
- * double; z (n_freq) complex128; grad_sigma / grad_eps_r (n_cells) double,
- * either may be NULL. */
+ * with the closed-form dca, dcb of freq_adjoint.py:186-206 and s = eps_r (the
+ * reference's scaling, exact only for h = sigma dt / (2 eps) << 1) or, with
+ * GDN_CONTRACT_EXACT_LOSS in flags, s = eps_r (1 + h) (exact for any sigma).
+ * All arrays are DEVICE: e_fwd, lam (n_freq, n_cells) complex128; eps_r,
+ * sigma (n_cells) double; z (n_freq) complex128; grad_sigma / grad_eps_r
+ * (n_cells) double, either may be NULL. */
+#define GDN_CONTRACT_EXACT_LOSS 1
 int gdn_tm_adjoint_contract(int32_t n_cells, int32_t n_freq, double dt, double k_norm,
                             const void* e_fwd, const void* lam, const double* eps_r,
                             const double* sigma, const void* z, double* grad_sigma,
-                            double* grad_eps_r, void* stream);
+                            double* grad_eps_r, int32_t flags, void* stream);
 
 /* ------------------------------------------------------------------------ */
 /* Near-to-far-field projection (3D and 2D)                                 */
@@ -362,6 +365,73 @@ int gdn_ntff2d_project_grad(int32_t n_freq, int32_t n_pts, int32_t n_ang, int32_
                             const double* pos, const double* w, const double* k,
                             const double* angles, double eta0, const void* g_out, void* g_Jz,
                             void* g_Ez, void* stream);
+
+/* ---- Design surrogate (BF16 U-Net) kernels ----------------------------
+ * No reference counterpart (the reference has no learned component).
+ * Activations are NHWC bfloat16; a tensor may be the channel slice
+ * [c0, c0 + C) of a buffer whose rows hold `stride` channels. Weights are
+ * bfloat16 [taps * Cin][Cout], row k = tap * Cin + ci with
+ * tap = (dy + 1) * 3 + (dx + 1) (taps = 9) or 0 (taps = 1); zero padding. */
+
+/* out = act(bias + conv(in, w)): bf16 `out` (slice) and/or float32 `out32`
+ * (dense [P][Cout]); bias float32 or NULL; relu 0/1 selects the leaky ReLU
+ * act(x) = x > 0 ? x : slope x (slope 0 = ReLU). With `mask` non-NULL,
+ * outputs whose mask entry is <= 0 are multiplied by slope (the activation
+ * derivative when this is an input-gradient convolution). */
+int gdn_sur_conv_fwd(const void* in, int32_t in_stride, int32_t in_c0, int32_t N, int32_t H,
+                     int32_t W, int32_t Cin, int32_t taps, const void* w, const float* bias,
+                     int32_t Cout, int32_t relu, float slope, void* out, int32_t out_stride,
+                     int32_t out_c0,
+                     float* out32, const void* mask, int32_t mask_stride, int32_t mask_c0,
+                     void* stream);
+
+/* dw[k][co] += sum_p im2col(in)[p][k] g[p][co] and db[co] += sum_p g[p][co]
+ * (float32, accumulated; db may be NULL). */
+int gdn_sur_conv_wgrad(const void* in, int32_t in_stride, int32_t in_c0, int32_t N, int32_t H,
+                       int32_t W, int32_t Cin, int32_t taps, const void* g, int32_t g_stride,
+                       int32_t g_c0, int32_t Cout, float* dw, float* db, void* stream);
+
+/* Weights of the input-gradient convolution (Cin and Cout swapped, taps
+ * point-reflected): wt[(taps-1-tap) * Cout + co][ci] = w[tap * Cin + ci][co]. */
+int gdn_sur_flip_weights(const void* w, int32_t Cin, int32_t Cout, int32_t taps, void* wt,
+                         void* stream);
+
+/* 2x2 max pooling (H, W even) with the winning window position (uint8). */
+int gdn_sur_maxpool2(const void* in, int32_t in_stride, int32_t in_c0, int32_t N, int32_t H,
+                     int32_t W, int32_t C, void* out, void* arg, void* stream);
+
+/* gin[winner] += gout for the pooling of an (N, H, W, C) slice. */
+int gdn_sur_maxpool2_grad_acc(const void* gout, const void* arg, int32_t N, int32_t H,
+                              int32_t W, int32_t C, void* gin, int32_t gin_stride,
+                              int32_t gin_c0, void* stream);
+
+/* Nearest x2 upsampling of a dense (N, H, W, C) tensor into a slice, and the
+ * gradient (sum of the four copies) back to a dense (N, H, W, C) tensor. */
+int gdn_sur_upsample2(const void* in, int32_t N, int32_t H, int32_t W, int32_t C, void* out,
+                      int32_t out_stride, int32_t out_c0, void* stream);
+int gdn_sur_upsample2_grad(const void* gout, int32_t g_stride, int32_t g_c0, int32_t N,
+                           int32_t H, int32_t W, int32_t C, void* gin, void* stream);
+
+/* Head loss gradient for out32 (N, HW, C >= 3): channels 0, 1 = field,
+ * channel 2 = power density (predicted power = its mean over HW, written to
+ * mean[N]). With targets, L = wf mean (out[:2] - target_field)^2 +
+ * wp mean_n (mean_n - target_power_n)^2 is added to *loss (may be NULL);
+ * without (both NULL), grad = d(sum_n power_weight_n mean_n)/d out
+ * (power_weight NULL = 1). Writes the bf16 gradient (N, HW, C). */
+int gdn_sur_head_grad(const float* out32, int32_t N, int32_t HW, int32_t C,
+                      const float* target_field, const float* target_power,
+                      const float* power_weight, float wf, float wp, float* mean, void* grad,
+                      float* loss, void* stream);
+
+/* One Adam step on float32 master weights w (n) with gradient g and moments
+ * m, v, refreshing the bf16 copy w16 (may be NULL). hyper (device float[4])
+ * = {step, lr, 1 - b1^step, 1 - b2^step}: the step count is advanced on the
+ * device, so the call can be captured in a CUDA graph. */
+int gdn_sur_adam(float* w, const float* g, float* m, float* v, void* w16, int64_t n,
+                 float* hyper, float b1, float b2, float eps, void* stream);
+
+/* float32 -> bfloat16 conversion of n elements. */
+int gdn_sur_to_bf16(const float* a, void* b, int64_t n, void* stream);
 
 #ifdef __cplusplus
 }

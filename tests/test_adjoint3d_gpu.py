@@ -162,7 +162,11 @@ def test_flux_sigma_and_two_tones_match_fd():
 
     grid = _grid()
     sig0 = 0.02 * np.ones(DR_SHAPE)
-    for freqs, tol in (((F0,), 1e-2), ((3.4e9, 4.6e9), 2e-2)):
+    # With the exact loss factor the single-tone case carries the turn-on
+    # transient's +1.1% scale error (the reference's eps_r-only scaling
+    # happened to offset it by -0.65% at this sigma): 1.5e-2, the reference's
+    # bar for its single-point objectives.
+    for freqs, tol in (((F0,), 1.5e-2), ((3.4e9, 4.6e9), 2e-2)):
         cur, env = _cw(grid, freqs)
 
         def obj(ph):
@@ -195,6 +199,33 @@ def test_s11_sigma_matches_fd_and_port_regions():
     assert rel <= 1e-2, f"S11/sigma directional rel. error {rel:.2e} ({a} vs {b})"
     g_reg = _adjoint(grid, obj, "sigma", sig0, env, common, objective_kind="port")
     assert np.allclose(g_reg, g, rtol=1e-9, atol=1e-12 * np.abs(g).max())
+
+
+def test_s11_lossy_design_exact_contraction():
+    """Design conductivities up to 30 S/m (c_a < 0): the exact contraction
+    (loss factor 1 + h, port kept as a load in the adjoint run) matches FD;
+    the reference's formula (exact=False) is off by several percent."""
+    import gradenna_b200 as gb
+    from gradenna_b200.sparams import s11_power_wave
+
+    grid = _grid()
+    cur, env = _cw(grid)
+    port = (10, 15, 15)
+
+    def obj(ph):
+        s = s11_power_wave(ph.port_v[0, 0], ph.port_i[0, 0], 50.0)
+        return s.real**2 + s.imag**2
+
+    common = dict(design_region=DR, dft_freqs=(F0,), port_ijk=port, port_voltage=cur,
+                  port_resistance=50.0, cpml=gb.CPMLSpec(NPML))
+    sig0 = np.random.default_rng(0).uniform(0, 30, DR_SHAPE)
+    g = _adjoint(grid, obj, "sigma", sig0, env, common)
+    g_ref = _adjoint(grid, obj, "sigma", sig0, env, common, exact=False)
+    for seed in (0, 1):
+        rel, a, b = _directional(grid, obj, "sigma", sig0, common, g, port=port, seed=seed)
+        assert rel <= 1.5e-2, f"S11 lossy directional rel. error {rel:.2e} ({a} vs {b})"
+        rel_ref, _, _ = _directional(grid, obj, "sigma", sig0, common, g_ref, port=port, seed=seed)
+        assert rel_ref > 3 * rel
 
 
 def test_ntff_directivity_matches_fd_and_box_regions():

@@ -176,3 +176,29 @@ def test_zero_steps_and_bad_args():
         gb.simulate_tm(g, source_ij=(0, 10), source_current=np.zeros(5), cpml=gb.CPMLSpec(4))
     with pytest.raises(ValueError):
         gb.simulate_tm(g, source_ij=(10, 10), source_current=np.zeros(5), cpml=gb.CPMLSpec(9))
+
+
+@pytest.mark.parametrize("dtype", [np.float64, np.float32])
+def test_heterogeneous_eps_sigma_and_metal(dtype):
+    """Media beyond the reference's native cases: eps_r in [1, 4] and sigma
+    from lossy (up to 5 S/m, where c_a turns negative) to metal (1e5 S/m),
+    with a source, a probe and a DFT."""
+    import gradenna_b200 as gb
+
+    g = ref.Grid2D(48, 44, 1e-3, 1e-3)
+    rng = np.random.default_rng(4)
+    n_steps = 600
+    src = _gauss(g, n_steps, dtype)
+    eps_r = 1.0 + 3.0 * rng.uniform(0, 1, (48, 44))
+    sigma = 10.0 ** (-4 + 9 * rng.uniform(0, 1, (48, 44)))
+    sigma[:, :20] = rng.uniform(0, 5, (48, 20))
+    kw = dict(source_ij=(24, 30), source_current=src, probe_ij=((12, 14), (30, 34)),
+              dft_freqs=(3e9,))
+    r_gpu, r_ref, r_64 = _run_both(
+        dtype, g, dict(kw, eps_r=eps_r, sigma=sigma, cpml=ref.CPMLSpec(8)),
+        dict(kw, eps_r=torch.as_tensor(eps_r), sigma=torch.as_tensor(sigma),
+             cpml=gb.CPMLSpec(8)))
+    for name in ("probe_ez", "dft_ez", "dft_hx", "dft_hy"):
+        assert rel(getattr(r_gpu, name), getattr(r_ref, name)) <= RTOL[dtype], name
+        assert rel(getattr(r_gpu, name), getattr(r_64, name)) <= 1e-3, name
+    assert rel(r_gpu.ez, r_ref.ez) <= RTOL_FIELD[dtype]
