@@ -435,9 +435,9 @@ def optimize_plain(problem: AntennaProblem, *, n_iters: int = 200,
 
 
 def optimize_surrogate(problem: AntennaProblem, surrogate: Surrogate | None, *,
-                       n_outer: int = 24, n_inner: int = 30, inner_lrs=(0.15, 0.5),
-                       betas=(8.0, 16.0, 32.0, 64.0), use_network: bool = True,
-                       target: float | None = None, device=None,
+                       n_outer: int = 24, n_inner: int = 30, inner_lrs=(0.1, 0.3, 1.0),
+                       betas=(8.0, 16.0, 32.0, 64.0), iters_per_beta: int = 3,
+                       use_network: bool = True, target: float | None = None, device=None,
                        tile_config: int | None = None) -> dict:
     """The batched+surrogate optimiser (see the module docstring).
 
@@ -450,9 +450,10 @@ def optimize_surrogate(problem: AntennaProblem, surrogate: Surrogate | None, *,
     if it improves the verified fraction (its adjoint run then gives the next
     gradient, and if it used the largest step size the step sizes grow by
     1.5x); otherwise the step sizes halve. The beta stage advances every
-    n_outer / len(betas) outer iterations (the current design is re-verified
-    at the new beta). With ``target``, the loop stops once a verified design
-    at the final beta reaches it. Returns "fraction" / "seconds" /
+    ``iters_per_beta`` outer iterations up to the last one, which then holds
+    for the remaining iterations (the current design is re-verified at each
+    new beta). With ``target``, the loop stops once a verified design at the
+    final beta reaches it. Returns "fraction" / "seconds" /
     "fdtd_runs" per outer iteration (the accepted design's verified
     fraction), "beta", "accepted" (model of the accepted candidate, or ""),
     "theta", "rho".
@@ -468,7 +469,7 @@ def optimize_surrogate(problem: AntennaProblem, surrogate: Surrogate | None, *,
     B = int(use_net.numel())
     n_net = int(use_net.sum())
     scale = 1.0
-    sched = beta_schedule(betas, max(1, n_outer // len(betas)))
+    sched = beta_schedule(betas, max(1, int(iters_per_beta)))
     fr, secs, runs, bh, acc = [], [], [], [], []
     n_runs = 0
     t0 = _clock(dev)
