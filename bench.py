@@ -89,7 +89,7 @@ P3_PHIS = tuple(np.linspace(0.0, 2 * np.pi, 16, endpoint=False))
 # design, 7000 steps, 2.45 GHz CW port drive); the plain optimiser runs 200
 # Adam iterations (beta 8 -> 64), the batched+surrogate optimiser runs until
 # a verified design at beta 64 reaches the plain optimiser's final value.
-SUR_SAMPLES = 4096
+SUR_SAMPLES = 8192
 SUR_EPOCHS = 30
 SUR_PLAIN_ITERS = 200
 SUR_OUTER = 24
@@ -105,7 +105,8 @@ def parse():
     ap.add_argument("--grid", type=int, default=N_GRID)
     ap.add_argument("--time-steps", type=int, default=None,
                     help="time steps per run (default: 8000 for tm2d, 6000 for patch3d)")
-    ap.add_argument("--workload", choices=("tm2d", "patch3d", "population", "surrogate"),
+    ap.add_argument("--workload",
+                    choices=("tm2d", "patch3d", "population", "surrogate", "unet"),
                     default="tm2d")
     ap.add_argument("--samples", type=int, default=SUR_SAMPLES,
                     help="surrogate workload: training designs solved by the batched kernel")
@@ -114,7 +115,7 @@ def parse():
     args = ap.parse_args()
     if args.time_steps is None:
         args.time_steps = {"tm2d": N_STEPS, "patch3d": P3_STEPS, "population": 0,
-                           "surrogate": 0}[args.workload]
+                           "surrogate": 0, "unet": 0}[args.workload]
     return args
 
 
@@ -447,6 +448,10 @@ def dist_setup(args):
 def run_reference(args):
     world, rank, _ = dist_setup(args)
     if rank != 0:
+        return 0
+    if args.workload == "unet":
+        print(json.dumps({"impl": "reference", "unavailable": "the reference has no learned "
+                          "surrogate, so there is no U-Net training step to time"}), flush=True)
         return 0
     if args.workload == "surrogate":
         P, spec = _hero_cpu_spec()
@@ -819,7 +824,7 @@ def run_surrogate(args):
     P = S.AntennaProblem()
     # Offline: training data from the batched kernel, then training.
     data = S.generate_dataset(P, args.samples, seed=rank, device=dev)
-    sur, hist = S.train_surrogate(data, epochs=args.epochs, device=dev)
+    sur, hist = S.train_surrogate(data, epochs=args.epochs, lr=5e-4, device=dev)
     fwd_flops = 2 * sum(
         ly.taps * ly.cin * ly.cout * (P.design_shape[0] >> _unet_level(ly.name))
         * (P.design_shape[1] >> _unet_level(ly.name)) for ly in sur.net.layers)
@@ -902,6 +907,114 @@ def run_surrogate(args):
                     "d2h_bytes_per_step": 0,
                     "note": "the optimisers are host-driven end to end; value is their "
                             "synchronised wall time"},
+            "gpu_launches": int(launches),
+            "clocks": clk.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if pg is not None:
+        pg.barrier()
+        pg.destroy_process_group()
+    return 0
+
+
+UNET_BATCH = 32
+
+
+def unet_step_flops(net) -> float:
+    """Convolution FLOPs of one training step: forward, input gradients
+    (all but the first layer) and weight gradients, 2 per multiply-add."""
+    spec = net.spec
+    total = 0.0
+    for ly in net.layers:
+        lev = _unet_level(ly.name)
+        px = (spec.height >> lev) * (spec.width >> lev)
+        f = 2.0 * px * ly.taps * ly.cin * ly.cout
+        total += f * (2 if ly.name == "enc0a" else 3)
+    return total
+
+
+def run_unet(args):
+    """Training step of the 104 x 104 surrogate U-Net (batch 32) on its own
+    BF16 tensor-core kernels: forward, head loss, backward, Adam."""
+    import torch
+
+    from gradenna_b200 import _native
+    from gradenna_b200.unet import UNet, UNetSpec
+
+    world, rank, local = dist_setup(args)
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    pg = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120), device_id=dev)
+        pg = dist
+    spec = UNetSpec()
+    net = UNet(spec, seed=rank, device=dev, learning_rate=1e-4)
+    g = torch.Generator(device="cpu").manual_seed(rank)
+    n = UNET_BATCH
+    x_h = torch.rand((n, spec.height, spec.width), generator=g).pin_memory()
+    tf_h = torch.randn((n, spec.height, spec.width, 2), generator=g).pin_memory()
+    tp_h = torch.rand((n,), generator=g).pin_memory()
+    x, tf, tp = x_h.to(dev), tf_h.to(dev), tp_h.to(dev)
+    loss_h = torch.empty((), dtype=torch.float32).pin_memory()
+    flops = unet_step_flops(net) * n
+    for _ in range(args.warmup):
+        net.train_step(x, tf, tp)
+    torch.cuda.synchronize()
+    if pg is not None:
+        pg.barrier()
+    stream = torch.cuda.current_stream(dev)
+    l0 = _native.kernel_launches()
+    with ClockSampler(local) as clk:
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(args.steps):
+            net.train_step(x, tf, tp)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t_step = e0.elapsed_time(e1) / 1e3 / args.steps
+        launches = (_native.kernel_launches() - l0) // args.steps
+        # e2e: the batch copied in from pinned host memory, the loss read back.
+        e0.record(stream)
+        for _ in range(args.steps):
+            xd = x_h.to(dev, non_blocking=True)
+            tfd = tf_h.to(dev, non_blocking=True)
+            tpd = tp_h.to(dev, non_blocking=True)
+            loss_h.copy_(net.train_step(xd, tfd, tpd), non_blocking=True)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        t_e2e = e0.elapsed_time(e1) / 1e3 / args.steps
+    t_step, t_e2e = max_over_ranks(pg, [t_step, t_e2e], dev)
+    if rank == 0:
+        try:
+            peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+            peak, kind = float(peaks["bf16_tflops"]), "measured (cuBLAS bf16 burst)"
+        except (OSError, KeyError, ValueError):
+            peak, kind = 1590.0, "fallback"
+        value = world * flops / t_step / 1e12
+        line = {
+            "metric": "U-Net training TFLOP/s", "value": value, "unit": "TFLOP/s",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t_step * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "bf16", "data": "synthetic",
+            "config": {"workload": "surrogate U-Net training step: 104 x 104 densities, "
+                                   "4 levels, 32 base channels, batch 32, BF16 weights and "
+                                   "activations, FP32 accumulation and master weights, Adam",
+                       "params": net.n_params, "flops_per_step": flops,
+                       "parallelism": f"replicas x{world}",
+                       "l2": "inputs (35 MB of activations) below L2; not flushed"},
+            "roofline": {"bound": "tensor", "achieved": value / world, "peak": peak,
+                         "unit": "TFLOP/s", "frac": value / world / peak, "traffic": None,
+                         "kernel": "all convolution kernels of the step (conv_fwd, conv_wgrad) "
+                                   "plus their elementwise kernels", "peak_source": kind},
+            "cpu_baseline": None,
+            "e2e": {"value": world * flops / t_e2e / 1e12, "unit": "TFLOP/s",
+                    "h2d_bytes_per_step": int(x_h.nbytes + tf_h.nbytes + tp_h.nbytes),
+                    "d2h_bytes_per_step": 4},
             "gpu_launches": int(launches),
             "clocks": clk.summary(),
         }
@@ -1041,6 +1154,8 @@ def main():
         return run_population(args)
     if args.workload == "surrogate":
         return run_surrogate(args)
+    if args.workload == "unet":
+        return run_unet(args)
     return run_ours(args)
 
 

@@ -276,12 +276,18 @@ def generate_dataset(problem: AntennaProblem, n: int, *, seed: int = 0, batch: i
                      device=None, tile_config: int | None = None) -> dict:
     """n seeded densities solved by the batched FDTD kernel (forward runs).
 
-    Returns {"rho": (n, H, W) float32, "fraction": (n,) float32,
-    "ez": (n, H, W, 2) float32 (Re, Im of the design-region Ez phasor divided
-    by "ez_scale"), "ez_scale": float, "seconds": solve time}.
+    Feature radii are drawn from [1, 6] x the problem's filter radius, so the
+    designs have the same physical feature sizes at any cell size. Returns
+    {"rho": (n, H, W) float32, "fraction": (n,) float32, "ez": (n, H, W, 2)
+    float32 = asinh(Re, Im of the design-region Ez phasor / "ez_scale"),
+    "ez_scale": float (the median per-design RMS field), "seconds": solve
+    time}. The asinh keeps the few strongly driven designs from dominating
+    the field loss.
     """
     dev = _native.require_cuda(device)
-    rho = random_densities(n, problem.design_shape, seed=seed, device=dev)
+    r = problem.filter_radius
+    rho = random_densities(n, problem.design_shape, seed=seed, radius_range=(r, 6.0 * r),
+                           device=dev)
     frac = torch.empty(n, dtype=torch.float64, device=dev)
     ez = torch.empty((n,) + problem.design_shape, dtype=torch.complex128, device=dev)
     torch.cuda.synchronize(dev)
@@ -293,8 +299,9 @@ def generate_dataset(problem: AntennaProblem, n: int, *, seed: int = 0, batch: i
         ez[s:s + batch] = e
     torch.cuda.synchronize(dev)
     seconds = time.perf_counter() - t0
-    scale = float(torch.sqrt(torch.mean(ez.abs() ** 2)))
-    ez_ri = torch.stack([ez.real, ez.imag], dim=-1) / scale
+    rms = torch.sqrt(torch.mean(ez.abs() ** 2, dim=(1, 2)))
+    scale = float(torch.median(rms)) or 1.0
+    ez_ri = torch.asinh(torch.stack([ez.real, ez.imag], dim=-1) / scale)
     return {"rho": rho, "fraction": frac.to(torch.float32), "ez": ez_ri.to(torch.float32),
             "ez_scale": scale, "seconds": seconds}
 
@@ -303,7 +310,7 @@ class Surrogate:
     """A trained U-Net with the scaling of its outputs: channel 2's mean is
     (log(fraction + power_floor) - power_mean) / power_std (the radiated
     fraction of random designs spans orders of magnitude), channels 0, 1 are
-    Ez / ez_scale."""
+    asinh(Ez / ez_scale)."""
 
     def __init__(self, net: UNet, power_mean: float = 0.0, power_std: float = 1.0,
                  ez_scale: float = 1.0, power_floor: float = 1e-6):
@@ -316,7 +323,7 @@ class Surrogate:
     def predict(self, rho):
         """(fraction (B,), ez (B, H, W) complex) predicted for densities rho."""
         out, p = self.net.forward(torch.as_tensor(rho, dtype=torch.float32))
-        ez = torch.complex(out[..., 0], out[..., 1]) * self.ez_scale
+        ez = torch.complex(torch.sinh(out[..., 0]), torch.sinh(out[..., 1])) * self.ez_scale
         return self._fraction(p), ez
 
     def fraction_grad(self, rho, weight=None):
