@@ -57,6 +57,18 @@ _native.register("gdn_sur_head_grad", ctypes.c_int,
 _native.register("gdn_sur_adam", ctypes.c_int,
                  [_v, _v, _v, _v, _v, ctypes.c_int64, _v, _f, _f, _f, _v])
 _native.register("gdn_sur_to_bf16", ctypes.c_int, [_v, _v, ctypes.c_int64, _v])
+_native.register("gdn_sur_conv_fwd_tc", ctypes.c_int,
+                 [_v, _i, _i, _i, _i, _i, _i, _i, _v, _v, _i, _i, _f, _v, _i, _i, _v, _v, _i, _i, _v])
+_native.register("gdn_sur_weights_kmajor", ctypes.c_int, [_v, _i, _i, _i, _i, _v, _v])
+_native.register("gdn_sur_status", ctypes.c_int, [ctypes.POINTER(ctypes.c_int32), _i])
+
+
+def tc_timeouts(reset: bool = True) -> int:
+    """Number of tensor-core convolutions that gave up on a bounded wait
+    since the last reset (gdn_sur_status); 0 in normal operation."""
+    v = ctypes.c_int32()
+    _native.check(_native.load().gdn_sur_status(ctypes.byref(v), int(reset)))
+    return int(v.value)
 
 
 @dataclass(frozen=True)
@@ -170,7 +182,8 @@ class UNet:
     """
 
     def __init__(self, spec: UNetSpec = UNetSpec(), *, seed: int = 0, device=None,
-                 learning_rate: float = 1e-3, betas=(0.9, 0.999), eps: float = 1e-8):
+                 learning_rate: float = 1e-3, betas=(0.9, 0.999), eps: float = 1e-8,
+                 tensor_cores: bool | None = None):
         self.dev = _native.require_cuda(device)
         self.lib = _native.load()
         self.spec = spec
@@ -180,6 +193,17 @@ class UNet:
         self.theta = torch.as_tensor(self.init_params(spec, seed), **f32)
         self.theta16 = torch.zeros(self.n_params, dtype=torch.bfloat16, device=self.dev)
         self.flip16 = torch.zeros(self.n_params, dtype=torch.bfloat16, device=self.dev)
+        # K-major copies for the tcgen05 convolutions: forward and flipped.
+        self.wk16 = torch.zeros(self.n_params, dtype=torch.bfloat16, device=self.dev)
+        self.fk16 = torch.zeros(self.n_params, dtype=torch.bfloat16, device=self.dev)
+        if tensor_cores is None:
+            import os
+
+            # The tcgen05 convolutions are opt-in until they outrun the
+            # mma.sync ones (measured: 7.0 against 5.2 ms per training step).
+            tensor_cores = os.environ.get("GDN_SUR_TC", "0") == "1"
+        self.tensor_cores = bool(tensor_cores)
+        self._kmajor = False
         self.grad = torch.zeros(self.n_params, **f32)
         self.m = torch.zeros(self.n_params, **f32)
         self.v = torch.zeros(self.n_params, **f32)
@@ -212,6 +236,7 @@ class UNet:
             _native.check(self.lib.gdn_sur_to_bf16(self.theta.data_ptr(), self.theta16.data_ptr(),
                                                    self.n_params, self._s()))
         self._flipped = False
+        self._kmajor = False
 
     def set_learning_rate(self, lr: float) -> None:
         self.hyper[1].fill_(float(lr))
@@ -242,8 +267,15 @@ class UNet:
         st, sc0 = src
         dt_, dc0 = dst if dst is not None else (None, 0)
         mt, mc0 = mask if mask is not None else (None, 0)
-        _native.check(self.lib.gdn_sur_conv_fwd(
-            st.data_ptr(), st.shape[-1], sc0, n, h, w, cin, ly.taps, self._w16(ly, transpose),
+        use_tc = (self.tensor_cores and cin % 8 == 0 and st.shape[-1] % 8 == 0 and sc0 % 8 == 0
+                  and cout >= 8)
+        fn = self.lib.gdn_sur_conv_fwd_tc if use_tc else self.lib.gdn_sur_conv_fwd
+        if use_tc:
+            wbase = (self.fk16 if transpose else self.wk16).data_ptr() + 2 * ly.w_off
+        else:
+            wbase = self._w16(ly, transpose)
+        _native.check(fn(
+            st.data_ptr(), st.shape[-1], sc0, n, h, w, cin, ly.taps, wbase,
             None if transpose else self._bias(ly), cout, int(ly.relu and not transpose),
             float(self.spec.neg_slope), _native.ptr(dt_), 0 if dt_ is None else dt_.shape[-1], dc0, _native.ptr(out32),
             _native.ptr(mt), 0 if mt is None else mt.shape[-1], mc0, stream))
@@ -260,7 +292,19 @@ class UNet:
         for ly in self.layers:
             _native.check(self.lib.gdn_sur_flip_weights(self._w16(ly), ly.cin, ly.cout, ly.taps,
                                                         self._w16(ly, True), stream))
+            if self.tensor_cores:
+                _native.check(self.lib.gdn_sur_weights_kmajor(
+                    self._w16(ly), ly.cin, ly.cout, ly.taps, 1,
+                    self.fk16.data_ptr() + 2 * ly.w_off, stream))
         self._flipped = True
+
+    def _kmajor_all(self, stream) -> None:
+        if self.tensor_cores:
+            for ly in self.layers:
+                _native.check(self.lib.gdn_sur_weights_kmajor(
+                    self._w16(ly), ly.cin, ly.cout, ly.taps, 0,
+                    self.wk16.data_ptr() + 2 * ly.w_off, stream))
+        self._kmajor = True
 
     def workspace(self, n: int) -> _Ws:
         ws = self._ws.get(n)
@@ -272,6 +316,8 @@ class UNet:
     def _forward(self, ws: _Ws, stream) -> None:
         spec, lib, L, n = self.spec, self.lib, self.spec.levels, ws.n
         B = self.by_name
+        if not self._kmajor:
+            self._kmajor_all(stream)
         h0, w0 = spec.size(0)
         _native.check(lib.gdn_sur_to_bf16(ws.x32.data_ptr(), ws.x[0].data_ptr(), n * h0 * w0,
                                           stream))
@@ -395,6 +441,7 @@ class UNet:
                 self.theta16.data_ptr(), self.n_params, self.hyper.data_ptr(), self.betas[0],
                 self.betas[1], self.eps, s))
             self._flipped = False
+            self._kmajor = False
             return ws.loss.clone()[0]
 
     def gradients(self, x, target_field, target_power, *, field_weight: float = 1.0,

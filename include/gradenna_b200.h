@@ -433,6 +433,29 @@ int gdn_sur_adam(float* w, const float* g, float* m, float* v, void* w16, int64_
 /* float32 -> bfloat16 conversion of n elements. */
 int gdn_sur_to_bf16(const float* a, void* b, int64_t n, void* stream);
 
+/* gdn_sur_conv_fwd on the tcgen05 tensor cores (TMEM accumulators, 128-pixel
+ * tiles, 128-byte-swizzled K-major operands staged by cp.async). Same
+ * arguments and results, except the weights `wk` are K-major: [Cout][K]
+ * (see gdn_sur_weights_kmajor). Needs Cin, in_stride and in_c0 multiples of
+ * 8 and 16-byte aligned `in` and `wk`. Its mbarrier waits are bounded; a
+ * wait that runs out is recorded for gdn_sur_status. */
+int gdn_sur_conv_fwd_tc(const void* in, int32_t in_stride, int32_t in_c0, int32_t N, int32_t H,
+                        int32_t W, int32_t Cin, int32_t taps, const void* wk, const float* bias,
+                        int32_t Cout, int32_t relu, float slope, void* out, int32_t out_stride,
+                        int32_t out_c0, float* out32, const void* mask, int32_t mask_stride,
+                        int32_t mask_c0, void* stream);
+
+/* K-major weights for gdn_sur_conv_fwd_tc from [taps * Cin][Cout] weights w:
+ * flip = 0: the layer's own convolution, wk[co][tap * Cin + ci];
+ * flip = 1: its input-gradient convolution (Cin and Cout swapped, taps
+ * point-reflected), wk[ci][(taps - 1 - tap) * Cout + co]. */
+int gdn_sur_weights_kmajor(const void* w, int32_t Cin, int32_t Cout, int32_t taps, int32_t flip,
+                           void* wk, void* stream);
+
+/* Number of tensor-core convolutions whose bounded waits ran out since the
+ * last reset (0 in normal operation); synchronises with the device. */
+int gdn_sur_status(int32_t* timeouts, int32_t reset);
+
 #ifdef __cplusplus
 }
 #endif

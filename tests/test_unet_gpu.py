@@ -112,3 +112,76 @@ def test_training_reduces_loss():
     losses = [float(net.train_step(xs, tf, tp)) for _ in range(300)]
     assert np.all(np.isfinite(losses))
     assert np.mean(losses[-10:]) < 0.1 * np.mean(losses[:3])
+
+
+@pytest.mark.parametrize("cin,cout,taps,hw,n", [(32, 32, 9, (20, 28), 3), (64, 64, 9, (13, 13), 5),
+                                                (128, 256, 9, (26, 26), 2), (64, 32, 9, (52, 52), 1),
+                                                (256, 128, 1, (13, 13), 4), (32, 3, 1, (24, 24), 2),
+                                                (96, 40, 9, (17, 11), 2)])
+def test_tensor_core_conv_matches_mma_conv(cin, cout, taps, hw, n):
+    """gdn_sur_conv_fwd_tc (tcgen05, TMEM accumulators) against gdn_sur_conv_fwd
+    (mma.sync) on the same bf16 operands: channel slices in and out, bias,
+    leaky ReLU and the backward mask, ragged pixel counts and channel counts
+    that are not multiples of the tile; FP32 results within 2e-3 of the peak
+    (the two sum the same products in different orders)."""
+    import ctypes
+
+    from gradenna_b200 import _native
+    from gradenna_b200.unet import tc_timeouts
+
+    lib = _native.load()
+    h, w = hw
+    g = torch.Generator(device="cpu").manual_seed(cin * 7 + cout)
+    stride_in, c0_in = cin + 16, 8
+    x = torch.randn((n, h, w, stride_in), generator=g).to(torch.bfloat16).cuda()
+    wt = (torch.randn((taps * cin, cout), generator=g) / (taps * cin) ** 0.5).to(torch.bfloat16).cuda()
+    bias = torch.randn(cout, generator=g).cuda()
+    mask = torch.randn((n, h, w, cout), generator=g).to(torch.bfloat16).cuda()
+    wk = torch.empty_like(wt)
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    _native.check(lib.gdn_sur_weights_kmajor(wt.data_ptr(), cin, cout, taps, 0, wk.data_ptr(), s))
+    outs = []
+    tc_timeouts(reset=True)
+    for fn, wp in ((lib.gdn_sur_conv_fwd, wt), (lib.gdn_sur_conv_fwd_tc, wk)):
+        res = []
+        for relu, use_mask in ((1, False), (0, True)):
+            o16 = torch.zeros((n, h, w, cout + 8), dtype=torch.bfloat16, device="cuda")
+            o32 = torch.zeros((n * h * w, cout), dtype=torch.float32, device="cuda")
+            _native.check(fn(x.data_ptr(), stride_in, c0_in, n, h, w, cin, taps, wp.data_ptr(),
+                             bias.data_ptr(), cout, relu, 0.1, o16.data_ptr(), cout + 8, 8,
+                             o32.data_ptr(), mask.data_ptr() if use_mask else None,
+                             cout if use_mask else 0, 0, s))
+            res.append((o16, o32))
+        outs.append(res)
+    torch.cuda.synchronize()
+    assert tc_timeouts(reset=True) == 0
+    for (a16, a32), (b16, b32) in zip(outs[0], outs[1]):
+        scale = float(a32.abs().max())
+        assert float((a32 - b32).abs().max()) <= 2e-3 * scale
+        assert float((a16[..., 8:].float() - b16[..., 8:].float()).abs().max()) <= 1e-2 * scale
+        assert torch.equal(a16[..., :8], b16[..., :8])  # untouched channels
+
+
+def test_tensor_core_flipped_weights_give_input_gradient():
+    """gdn_sur_weights_kmajor(flip=1) + gdn_sur_conv_fwd_tc equals the
+    mma.sync input-gradient convolution with gdn_sur_flip_weights."""
+    import ctypes
+
+    from gradenna_b200 import _native
+
+    lib = _native.load()
+    cin, cout, taps, n, h, w = 64, 128, 9, 2, 26, 26
+    g = torch.Generator(device="cpu").manual_seed(3)
+    gy = torch.randn((n, h, w, cout), generator=g).to(torch.bfloat16).cuda()
+    wt = (torch.randn((taps * cin, cout), generator=g) / 24).to(torch.bfloat16).cuda()
+    flip = torch.empty_like(wt)
+    fk = torch.empty_like(wt)
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    _native.check(lib.gdn_sur_flip_weights(wt.data_ptr(), cin, cout, taps, flip.data_ptr(), s))
+    _native.check(lib.gdn_sur_weights_kmajor(wt.data_ptr(), cin, cout, taps, 1, fk.data_ptr(), s))
+    o = [torch.zeros((n * h * w, cin), dtype=torch.float32, device="cuda") for _ in range(2)]
+    for fn, wp, out in ((lib.gdn_sur_conv_fwd, flip, o[0]), (lib.gdn_sur_conv_fwd_tc, fk, o[1])):
+        _native.check(fn(gy.data_ptr(), cout, 0, n, h, w, cout, taps, wp.data_ptr(), None, cin, 0,
+                         0.1, None, 0, 0, out.data_ptr(), None, 0, 0, s))
+    torch.cuda.synchronize()
+    assert float((o[0] - o[1]).abs().max()) <= 2e-3 * float(o[0].abs().max())
