@@ -338,11 +338,15 @@ __global__ void weights_kmajor(const bf16* __restrict__ w, int Cin, int Cout, in
 template <int N>
 int launch(const Args& a, cudaStream_t s) {
   constexpr int smem = STAGES * (TM * 128 + N * 128) + 1024;
-  static bool configured = false;  // per process; the attribute is per function
-  if (!configured) {
+  // The dynamic shared-memory limit is a per-device function attribute.
+  static bool configured[64] = {};
+  int dev = 0;
+  GDN_TRY_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) GDN_BAD_ARG("device index %d out of range", dev);
+  if (!configured[dev]) {
     GDN_TRY_CUDA(cudaFuncSetAttribute(conv_fwd_tc<N>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                       smem));
-    configured = true;
+    configured[dev] = true;
   }
   const long long P = (long long)a.N * a.H * a.W;
   const dim3 grid(unsigned((P + TM - 1) / TM), unsigned((a.Cout + N - 1) / N));

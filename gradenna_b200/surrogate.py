@@ -341,13 +341,22 @@ class Surrogate:
 def train_surrogate(data: dict, *, spec: UNetSpec | None = None, epochs: int = 30,
                     batch: int = 32, lr: float = 1e-3, lr_final: float = 5e-5,
                     warmup: int = 300, field_weight: float = 1.0, power_weight: float = 4.0,
-                    val_fraction: float = 0.1, seed: int = 0, device=None) -> tuple:
+                    val_fraction: float = 0.1, seed: int = 0, device=None,
+                    data_parallel: bool = False) -> tuple:
     """Train a U-Net surrogate on ``generate_dataset`` output with its own
     CUDA kernels (linear warmup over ``warmup`` steps, then cosine decay from
     lr to lr_final). The power target is log(fraction + floor), floor = 1e-3
     of the largest fraction, standardised. Returns (Surrogate, history) with
     per-epoch training loss, the validation R^2 of the fraction and of its
-    log, the fraction RMSE and the field relative error, plus the time."""
+    log, the fraction RMSE and the field relative error, plus the time.
+
+    With ``data_parallel`` (inside an initialised torch.distributed process
+    group), every rank trains on its own data with the same initial weights
+    and the gradients are averaged over the ranks before each Adam step
+    (``unet.allreduce_mean``); the output scaling (log-fraction mean and
+    spread, field scale) is averaged the same way first, so all ranks hold
+    the same network. Every rank must take the same number of steps: pass
+    datasets of equal size.
     dev = _native.require_cuda(device)
     rho = data["rho"].to(dev)
     n, h, w = rho.shape
@@ -359,15 +368,35 @@ def train_surrogate(data: dict, *, spec: UNetSpec | None = None, epochs: int = 3
     perm = torch.randperm(n, generator=gen).to(dev)
     n_val = max(1, int(round(val_fraction * n))) if n > 1 else 0
     val, tr = perm[:n_val], perm[n_val:]
-    floor = max(1e-3 * float(frac.max()), 1e-30)
+    hook = None
+    ez_scale = data.get("ez_scale", 1.0)
+    fmax = float(frac.max())
+    if data_parallel:
+        import torch.distributed as dist
+
+        from gradenna_b200.unet import allreduce_mean
+
+        hook = allreduce_mean()
+        t = torch.tensor([fmax], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        fmax = float(t[0])
+    floor = max(1e-3 * fmax, 1e-30)
     lt = torch.log(frac.to(torch.float64) + floor)
     mu, sd = float(lt[tr].mean()), float(lt[tr].std()) or 1.0
+    if data_parallel:
+        t = torch.tensor([mu, sd, ez_scale], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        t /= dist.get_world_size()
+        mu, sd, common = float(t[0]), float(t[1]), float(t[2])
+        # re-express this rank's field targets in the common field scale
+        ez = torch.asinh(torch.sinh(ez.to(torch.float64)) * (ez_scale / common)).to(torch.float32)
+        ez_scale = common
     tp_all = ((lt - mu) / sd).to(torch.float32)
     steps_per_epoch = max(1, len(tr) // batch)
     total = epochs * steps_per_epoch
     warmup = min(warmup, max(1, total // 5))
     hist = {"loss": [], "val_rmse": [], "val_r2": [], "val_r2_log": [], "val_field_rel": []}
-    sur = Surrogate(net, mu, sd, data.get("ez_scale", 1.0), floor)
+    sur = Surrogate(net, mu, sd, ez_scale, floor)
     torch.cuda.synchronize(dev)
     t0 = time.perf_counter()
     step = 0
@@ -382,7 +411,7 @@ def train_surrogate(data: dict, *, spec: UNetSpec | None = None, epochs: int = 3
                 c = (step - warmup) / max(1, total - warmup)
                 net.set_learning_rate(lr_final + 0.5 * (lr - lr_final) * (1 + math.cos(math.pi * c)))
             acc += net.train_step(rho[idx], ez[idx], tp_all[idx], field_weight=field_weight,
-                                  power_weight=power_weight)
+                                  power_weight=power_weight, grad_hook=hook)
             step += 1
         hist["loss"].append(float(acc) / steps_per_epoch)
         if n_val:

@@ -39,7 +39,7 @@ import torch
 
 from gradenna_b200 import _native
 
-__all__ = ["UNetSpec", "Layer", "unet_layers", "UNet"]
+__all__ = ["UNetSpec", "Layer", "unet_layers", "UNet", "allreduce_mean", "tc_timeouts"]
 
 _v, _i, _f = ctypes.c_void_p, ctypes.c_int32, ctypes.c_float
 _native.register("gdn_sur_conv_fwd", ctypes.c_int,
@@ -69,6 +69,22 @@ def tc_timeouts(reset: bool = True) -> int:
     v = ctypes.c_int32()
     _native.check(_native.load().gdn_sur_status(ctypes.byref(v), int(reset)))
     return int(v.value)
+
+
+def allreduce_mean(group=None):
+    """A train_step gradient hook for data-parallel training: the sum of the
+    ranks' flat FP32 gradients over torch.distributed (NCCL over NVLink on
+    GPUs), divided by the world size, in place. Every rank then applies the
+    same Adam step, so the replicas stay identical."""
+    import torch.distributed as dist
+
+    world = dist.get_world_size(group)
+
+    def hook(grad):
+        dist.all_reduce(grad, op=dist.ReduceOp.SUM, group=group)
+        grad.div_(world)
+
+    return hook
 
 
 @dataclass(frozen=True)
@@ -415,11 +431,14 @@ class UNet:
         return out, out[..., 2].mean(dim=(1, 2))
 
     def train_step(self, x, target_field, target_power, *, field_weight: float = 1.0,
-                   power_weight: float = 1.0):
+                   power_weight: float = 1.0, grad_hook=None):
         """One Adam step on the loss
         field_weight * mean (out[..., :2] - target_field)^2
         + power_weight * mean_n (mean_hw out[..., 2] - target_power)^2.
-        Returns the loss before the step as a device scalar (no host sync)."""
+        Returns the loss before the step as a device scalar (no host sync).
+        ``grad_hook(grad)`` runs between the backward pass and Adam on the
+        flat FP32 gradient (in place): data-parallel training passes the
+        all-reduce mean over the ranks there (``allreduce_mean``)."""
         with torch.cuda.device(self.dev):
             ws = self._load_input(x)
             tf = torch.as_tensor(target_field, dtype=torch.float32, device=self.dev).contiguous()
@@ -436,6 +455,8 @@ class UNet:
                 tp.data_ptr(), None, float(field_weight), float(power_weight),
                 ws.mean.data_ptr(), ws.g_out.data_ptr(), ws.loss.data_ptr(), s))
             self._backward(ws, s, weights=True, input_grad=False)
+            if grad_hook is not None:
+                grad_hook(self.grad)
             _native.check(self.lib.gdn_sur_adam(
                 self.theta.data_ptr(), self.grad.data_ptr(), self.m.data_ptr(), self.v.data_ptr(),
                 self.theta16.data_ptr(), self.n_params, self.hyper.data_ptr(), self.betas[0],
