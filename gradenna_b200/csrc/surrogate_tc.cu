@@ -383,8 +383,19 @@ extern "C" int gdn_sur_conv_fwd_tc(const void* in, int32_t in_stride, int32_t in
          static_cast<const bf16*>(wk), bias, Cout, relu, slope, static_cast<bf16*>(out),
          out_stride, out_c0, out32, static_cast<const bf16*>(mask), mask_stride, mask_c0};
   cudaStream_t s = static_cast<cudaStream_t>(stream);
-  if (Cout <= 32) return launch<32>(a, s);
-  if (Cout <= 64) return launch<64>(a, s);
+  // Channel tile: the smallest of 32 / 64 / 128 covering Cout, narrowed while
+  // the grid holds fewer than two CTAs per SM (the coarse U-Net levels have
+  // few pixels), since one 128-thread CTA cannot keep an SM's tensor core fed.
+  static int sms[64] = {};
+  int dev = 0;
+  GDN_TRY_CUDA(cudaGetDevice(&dev));
+  if (dev < 0 || dev >= 64) GDN_BAD_ARG("device index %d out of range", dev);
+  if (!sms[dev]) GDN_TRY_CUDA(cudaDeviceGetAttribute(&sms[dev], cudaDevAttrMultiProcessorCount, dev));
+  const long long mtiles = ((long long)N * H * W + TM - 1) / TM;
+  int n = Cout <= 32 ? 32 : (Cout <= 64 ? 64 : 128);
+  while (n > 32 && mtiles * ((Cout + n - 1) / n) < 2LL * sms[dev]) n /= 2;
+  if (n == 32) return launch<32>(a, s);
+  if (n == 64) return launch<64>(a, s);
   return launch<128>(a, s);
 }
 

@@ -357,6 +357,7 @@ def train_surrogate(data: dict, *, spec: UNetSpec | None = None, epochs: int = 3
     spread, field scale) is averaged the same way first, so all ranks hold
     the same network. Every rank must take the same number of steps: pass
     datasets of equal size.
+    """
     dev = _native.require_cuda(device)
     rho = data["rho"].to(dev)
     n, h, w = rho.shape
