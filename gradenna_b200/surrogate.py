@@ -89,8 +89,10 @@ class AntennaProblem:
 
     @classmethod
     def coarse(cls) -> "AntennaProblem":
-        """The same physical layout at 3 mm cells: 96 x 96 grid, 32 x 32
-        design, 2400 steps (the same 16.8 ns), filter radius 2."""
+        """The same physical layout at 3 mm cells: 96 x 96 grid, 2400 steps
+        (the same 16.8 ns), filter radius 2 (the same 6 mm), and a 32 x 32
+        design (96 mm, a multiple of 8 cells for the U-Net, centred where
+        the hero's 104 mm region is)."""
         return cls(nx=96, ny=96, dx=3e-3, n_steps=2400, ramp_steps=240, port_ij=(47, 33),
                    design=(31, 63, 28, 60), flux_box=(13, 80, 13, 80), filter_radius=2.0)
 
