@@ -86,6 +86,8 @@ class AntennaProblem:
     sigma_min: float = 1e-4
     sigma_max: float = 1e5
     filter_radius: float = 6.0
+    drive_kind: str = "cw"  # "cw" (frequency-domain adjoint) or "pulse" (time-domain adjoint)
+    f_max: float = 3.5e9    # upper band edge of the pulse drive
 
     @classmethod
     def coarse(cls) -> "AntennaProblem":
@@ -115,9 +117,18 @@ class AntennaProblem:
         return (i1 - i0, j1 - j0)
 
     def drive(self):
-        """(v, env): the CW port voltage sampled at (n + 1/2) dt and its
-        raised-cosine turn-on envelope."""
+        """(v, env): the port voltage sampled at (n + 1/2) dt and its turn-on
+        envelope. CW: a 2.45 GHz sine under a raised-cosine ramp. Pulse: the
+        reference's band pulse gaussian_pulse_for_band(f_min, f_max)
+        (export_viz.py:136-138), envelope all ones (unused)."""
         n = np.arange(self.n_steps, dtype=np.float64)
+        if self.drive_kind == "pulse":
+            from gradenna_b200.sparams import gaussian_pulse_for_band
+
+            v = gaussian_pulse_for_band(self.f_min, self.f_max)((n + 0.5) * self.grid.dt)
+            return np.asarray(v, np.float64), np.ones(self.n_steps)
+        if self.drive_kind != "cw":
+            raise ValueError(f"drive_kind must be 'cw' or 'pulse', got {self.drive_kind!r}")
         env = np.where(n < self.ramp_steps, 0.5 - 0.5 * np.cos(np.pi * n / self.ramp_steps), 1.0)
         v = env * np.sin(2 * np.pi * self.f0 * (n + 0.5) * self.grid.dt)
         return v, env
@@ -156,7 +167,8 @@ class AntennaProblem:
 
 
 class _Judge:
-    """Cached plan and objective of a problem on a device."""
+    """Cached plan and objective of a problem on a device (and, for the
+    pulse drive, the time-domain adjoint plan)."""
 
     _cache: dict = {}
 
@@ -165,6 +177,19 @@ class _Judge:
         key = (problem, str(dev))
         if key not in cls._cache:
             cls._cache[key] = (problem.plan(dev), problem.objective())
+        return cls._cache[key]
+
+    @classmethod
+    def tplan(cls, problem: AntennaProblem, dev):
+        key = ("t", problem, str(dev))
+        if key not in cls._cache:
+            from gradenna_b200.time_adjoint import _TPlan
+
+            v, _ = problem.drive()
+            ports = (Port(tuple(problem.port_ij), problem.resistance, v.astype(np.float32)),)
+            cls._cache[key] = _TPlan(problem.grid, problem.design_region, (problem.f0,), None,
+                                     None, ports, problem.cpml, torch.float32, dev,
+                                     poynting_box_monitors(problem.flux_box))
         return cls._cache[key]
 
 
@@ -178,15 +203,21 @@ class _Forward:
 
 def forward_batch(problem: AntennaProblem, rhos, *, device=None,
                   tile_config: int | None = None) -> _Forward:
-    """Forward CW runs of designs ``rhos`` (B, H, W), batched; the result
-    holds the radiated fractions (B,) and design-region Ez phasors."""
+    """Forward runs of designs ``rhos`` (B, H, W), batched; the result holds
+    the radiated fractions (B,) and design-region Ez phasors (and, for the
+    pulse drive, the design cells' Ez histories for the time-domain
+    adjoint)."""
     dev = _native.require_cuda(device)
     plan, obj = _Judge.get(problem, dev)
     rhos = torch.as_tensor(rhos, device=dev).to(torch.float64).reshape((-1,) + problem.design_shape)
     designs = [fa._full_eps_sigma(problem.grid, problem.design_sigma(rho), None,
                                   problem.design_region, dev) for rho in rhos]
-    fwd = simulate_tm_batch([fa._forward_kwargs(plan, e, s) for e, s in designs],
-                            tile_config=tile_config, device=dev)
+    kws = [fa._forward_kwargs(plan, e, s) for e, s in designs]
+    if problem.drive_kind == "pulse":
+        cells = _Judge.tplan(problem, dev).cells  # design-cell Ez histories
+        for kw in kws:
+            kw["probe_ij"] = cells
+    fwd = simulate_tm_batch(kws, tile_config=tile_config, device=dev)
     full = [fa._scatter_full(plan, res) for res in fwd]
     fr = torch.stack([fa._objective_value(plan, obj, fu, res).detach().to(torch.float64).reshape(())
                       for fu, res in zip(full, fwd)])
@@ -196,15 +227,34 @@ def forward_batch(problem: AntennaProblem, rhos, *, device=None,
 
 def adjoint_batch(state: _Forward, which, *, tile_config: int | None = None) -> list:
     """Exact d fraction / d rho (H, W) float64 of the designs ``which`` of a
-    forward batch: their adjoint runs batched, then the contraction."""
+    forward batch: their adjoint runs batched, then the contraction (the
+    frequency-domain adjoint for the CW drive, the time-domain adjoint of
+    gradenna_b200.time_adjoint for the pulse drive)."""
     problem, dev = state.problem, state.dev
     plan, obj = _Judge.get(problem, dev)
+    pulse = problem.drive_kind == "pulse"
+    if pulse:
+        from gradenna_b200 import time_adjoint as ta
+
+        tp = _Judge.tplan(problem, dev)
     which = list(which)
     kws, at = [], []
     for k in which:
         e, s = state.designs[k]
         _, cot = fa._cotangents(plan, obj, state.full[k], state.fwd[k])
-        kw = fa._adjoint_kwargs(plan, e, s, fa._adjoint_sources(plan, cot))
+        if pulse:
+            jz_i, jz, mx_i, mx, my_i, my = ta._adjoint_sources(tp, cot)
+            kw = None
+            if jz_i is not None or mx_i is not None or my_i is not None:
+                kw = dict(grid=problem.grid, source_ij=jz_i,
+                          source_current=None if jz is None else jz.float(), mx_ij=mx_i,
+                          mx_current=None if mx is None else mx.float(), my_ij=my_i,
+                          my_current=None if my is None else my.float(), eps_r=e, sigma=s,
+                          ports=tuple(Port(p.ij, p.resistance, None) for p in tp.ports),
+                          probe_ij=tp.cells, cpml=problem.cpml, dtype=torch.float32,
+                          device=dev)
+        else:
+            kw = fa._adjoint_kwargs(plan, e, s, fa._adjoint_sources(plan, cot))
         if kw is not None:
             kws.append(kw)
             at.append(k)
@@ -216,8 +266,12 @@ def adjoint_batch(state: _Forward, which, *, tile_config: int | None = None) -> 
             out.append(torch.zeros(problem.design_shape, dtype=torch.float64, device=dev))
             continue
         e, s = state.designs[k]
-        gs, _ = fa._contract(plan, e, s, state.fwd[k].monitors[0], adj[at.index(k)].monitors[0],
-                             True, False)
+        if pulse:
+            gs = ta._contract(tp, e, ta._total_sigma(tp, s), state.fwd[k].probe_ez,
+                              adj[at.index(k)].probe_ez, True, False)["sigma"]
+        else:
+            gs, _ = fa._contract(plan, e, s, state.fwd[k].monitors[0],
+                                 adj[at.index(k)].monitors[0], True, False)
         # d sigma / d rho of sigma_from_density (zero on the feed cell).
         out.append(gs * s[problem.design_region] * (math.log(10.0) * (hi - lo)))
     return out
