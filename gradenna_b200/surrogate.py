@@ -290,15 +290,12 @@ def evaluate(problem: AntennaProblem, rhos, *, gradient: bool = True, device=Non
 
 def design_transform(theta: torch.Tensor, beta, radius: float, eta: float = 0.5) -> torch.Tensor:
     """theta (B, H, W) -> sigmoid -> conic filter -> tanh projection: the
-    batched form of topopt.DesignTransform (topopt.py:109-127)."""
-    rho = torch.sigmoid(theta)
-    if radius > 1.0:
-        k = torch.as_tensor(conic_kernel(radius, 2), dtype=rho.dtype, device=rho.device)
-        pad = k.shape[0] // 2
-        num = F.conv2d(rho[:, None], k[None, None], padding=pad)[:, 0]
-        den = F.conv2d(torch.ones_like(rho[:1, None]), k[None, None], padding=pad)[:, 0]
-        rho = num / den
-    return tanh_projection(rho, beta, eta)
+    batched form of topopt.DesignTransform (topopt.py:109-127), on the
+    library's fused kernels for float64 CUDA tensors
+    (topopt.design_transform_batch)."""
+    from gradenna_b200.topopt import design_transform_batch
+
+    return design_transform_batch(theta, beta, radius, eta)
 
 
 def random_densities(n: int, shape, *, seed: int = 0, radius_range=(2.0, 12.0),

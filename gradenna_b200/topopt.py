@@ -65,6 +65,84 @@ class DesignTransform:
         return tanh_projection(rho, beta, self.eta)
 
 
+def _register_design_entry_points():
+    import ctypes
+
+    from gradenna_b200 import _native
+
+    v, i, d = ctypes.c_void_p, ctypes.c_int32, ctypes.c_double
+    _native.register("gdn_design_forward", ctypes.c_int, [v, i, i, i, v, i, d, d, v, v, v, v])
+    _native.register("gdn_design_backward", ctypes.c_int,
+                     [v, v, v, v, i, i, i, v, i, d, d, v, v])
+
+
+_register_design_entry_points()
+
+
+class _DesignTransformCUDA(torch.autograd.Function):
+    """sigmoid -> conic filter -> tanh projection of a batch of float64
+    designs on the GPU (gdn_design_forward / gdn_design_backward)."""
+
+    @staticmethod
+    def forward(ctx, theta, beta, radius, eta):
+        import ctypes
+
+        from gradenna_b200 import _native
+
+        lib = _native.load()
+        th = theta.detach().contiguous()
+        B, H, W = th.shape
+        if radius > 1.0:
+            kern = torch.as_tensor(conic_kernel(radius, 2), dtype=torch.float64, device=th.device)
+        else:
+            kern = torch.ones((1, 1), dtype=torch.float64, device=th.device)
+        n = (kern.shape[0] - 1) // 2
+        filt, norm, rho = (torch.empty_like(th) for _ in range(3))
+        s = ctypes.c_void_p(torch.cuda.current_stream(th.device).cuda_stream)
+        with torch.cuda.device(th.device):
+            _native.check(lib.gdn_design_forward(th.data_ptr(), B, H, W, kern.data_ptr(), n,
+                                                 float(beta), float(eta), filt.data_ptr(),
+                                                 norm.data_ptr(), rho.data_ptr(), s))
+        ctx.save_for_backward(th, filt, norm, kern)
+        ctx.args = (float(beta), float(eta), n)
+        return rho
+
+    @staticmethod
+    def backward(ctx, g):
+        import ctypes
+
+        from gradenna_b200 import _native
+
+        th, filt, norm, kern = ctx.saved_tensors
+        beta, eta, n = ctx.args
+        g = g.contiguous().to(torch.float64)
+        out = torch.empty_like(th)
+        B, H, W = th.shape
+        s = ctypes.c_void_p(torch.cuda.current_stream(th.device).cuda_stream)
+        with torch.cuda.device(th.device):
+            _native.check(_native.load().gdn_design_backward(
+                th.data_ptr(), filt.data_ptr(), norm.data_ptr(), g.data_ptr(), B, H, W,
+                kern.data_ptr(), n, beta, eta, out.data_ptr(), s))
+        return out, None, None, None
+
+
+def design_transform_batch(theta: torch.Tensor, beta, radius: float,
+                           eta: float = 0.5) -> torch.Tensor:
+    """DesignTransform of a batch theta (B, H, W), differentiable. float64
+    CUDA tensors run the library's fused kernels (one launch forward, one
+    backward); other tensors run the torch form."""
+    if theta.is_cuda and theta.dtype == torch.float64 and theta.ndim == 3:
+        return _DesignTransformCUDA.apply(theta, float(beta), float(radius), float(eta))
+    rho = torch.sigmoid(theta)
+    if radius > 1.0:
+        k = torch.as_tensor(conic_kernel(radius, 2), dtype=rho.dtype, device=rho.device)
+        pad = k.shape[0] // 2
+        num = F.conv2d(rho[:, None], k[None, None], padding=pad)[:, 0]
+        den = F.conv2d(torch.ones_like(rho[:1, None]), k[None, None], padding=pad)[:, 0]
+        rho = num / den
+    return tanh_projection(rho, beta, eta)
+
+
 def beta_schedule(betas=(8.0, 16.0, 32.0, 64.0), steps_per_beta: int = 100):
     """beta continuation: iteration -> beta, one stage per ``steps_per_beta``
     iterations, holding the last stage afterwards (topopt.py:130-150)."""

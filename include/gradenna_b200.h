@@ -452,6 +452,21 @@ int gdn_sur_conv_fwd_tc(const void* in, int32_t in_stride, int32_t in_c0, int32_
 int gdn_sur_weights_kmajor(const void* w, int32_t Cin, int32_t Cout, int32_t taps, int32_t flip,
                            void* wk, void* stream);
 
+/* ---- Topology-optimisation design transform ----------------------------
+ * rho = tanh_projection(conic_filter(sigmoid(theta), R), beta, eta) for B
+ * designs of H x W cells (src/gradenna/topopt.py:55-127, which runs in jax).
+ * kern: the (2n+1)^2 conic weights max(0, 1 - |o| / R), n <= 24; the
+ * filter is renormalised by the in-bounds weight sum at the border. All
+ * arrays are DEVICE double, (B, H, W). The forward also writes the filtered
+ * field and the per-cell weight sum, which the backward reads to turn
+ * g_rho = dL/drho into g_theta = dL/dtheta. */
+int gdn_design_forward(const double* theta, int32_t B, int32_t H, int32_t W, const double* kern,
+                       int32_t n, double beta, double eta, double* filt, double* norm,
+                       double* rho, void* stream);
+int gdn_design_backward(const double* theta, const double* filt, const double* norm,
+                        const double* g_rho, int32_t B, int32_t H, int32_t W, const double* kern,
+                        int32_t n, double beta, double eta, double* g_theta, void* stream);
+
 /* Number of tensor-core convolutions whose bounded waits ran out since the
  * last reset (0 in normal operation); synchronises with the device. */
 int gdn_sur_status(int32_t* timeouts, int32_t reset);
