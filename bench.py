@@ -868,6 +868,8 @@ def run_surrogate(args):
                          f"antenna problem ({t_cpu:.1f} s), extrapolated to the plain "
                          f"optimiser's {SUR_PLAIN_ITERS} iterations"}
         line = {
+            # When the surrogate run never reaches the target, value is the
+            # whole run's time and config.surrogate.reached is false.
             "metric": "GPU-seconds to the plain optimiser's final radiated fraction",
             "value": t_sur, "unit": "s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": (t_sur + t_plain) * 1e3,
@@ -888,7 +890,8 @@ def run_surrogate(args):
                               "fdtd_runs": int(su["fdtd_runs"][-1]),
                               "accepted": [str(a) for a in su["accepted"]],
                               "trajectory": [float(f) for f in su["fraction"]]},
-                "speedup_vs_plain": t_plain / t_sur,
+                # only meaningful when the surrogate run reached the target
+                "speedup_vs_plain": (t_plain / t_sur) if len(hit) else None,
                 "linear_model_ablation": {"final_fraction": float(lin["fraction"][-1]),
                                           "seconds": float(lin["seconds"][-1]),
                                           "reached": bool(np.any(lin["fraction"] >= target))},
