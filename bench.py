@@ -940,6 +940,42 @@ def unet_step_flops(net) -> float:
     return total
 
 
+def cpu_sample_unet(target_s: float = 10.0, batch: int = 2):
+    """The oracle U-Net (torch float32 on the host cores, bf16 rounding off)
+    training step: forward, loss, autograd backward, for about target_s
+    seconds. Returns (TFLOP/s, steps, seconds, threads)."""
+    import torch
+
+    from gradenna_b200.unet import UNet, UNetSpec, unet_layers
+    from oracle.unet_torch import unet_loss
+
+    spec = UNetSpec()
+    layers, n = unet_layers(spec)
+    theta = torch.as_tensor(UNet.init_params(spec, 0)).requires_grad_(True)
+    g = torch.Generator().manual_seed(0)
+    x = torch.rand((batch, spec.height, spec.width), generator=g)
+    tf = torch.randn((batch, spec.height, spec.width, 2), generator=g)
+    tp = torch.rand(batch, generator=g)
+    lt = [tuple(ly) for ly in layers]
+
+    class _Net:  # unet_step_flops reads .spec and .layers
+        pass
+
+    net = _Net()
+    net.spec, net.layers = spec, layers
+    flops = unet_step_flops(net) * batch
+    steps, t0 = 0, time.perf_counter()
+    while True:
+        loss = unet_loss(theta, lt, spec.levels, x, tf, tp, bf16=False)
+        theta.grad = None
+        loss.backward()
+        steps += 1
+        el = time.perf_counter() - t0
+        if el >= target_s or steps >= 1000:
+            break
+    return flops * steps / el / 1e12, steps, el, torch.get_num_threads()
+
+
 def run_unet(args):
     """Training step of the 104 x 104 surrogate U-Net (batch 32) on its own
     BF16 tensor-core kernels: forward, head loss, backward, Adam."""
@@ -997,6 +1033,10 @@ def run_unet(args):
         t_e2e = e0.elapsed_time(e1) / 1e3 / args.steps
     t_step, t_e2e = max_over_ranks(pg, [t_step, t_e2e], dev)
     if rank == 0:
+        v_cpu, n_cpu, t_cpu, threads = cpu_sample_unet()
+        cpu = {"value": v_cpu, "unit": "TFLOP/s", "cores": threads, "kind": "port",
+               "sample": f"oracle U-Net (torch float32 on the host), {n_cpu} training steps "
+                         f"of batch 2 at 104^2 in {t_cpu:.1f} s"}
         try:
             peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
             peak, kind = float(peaks["bf16_tflops"]), "measured (cuBLAS bf16 burst)"
@@ -1018,7 +1058,7 @@ def run_unet(args):
                          "unit": "TFLOP/s", "frac": value / world / peak, "traffic": None,
                          "kernel": "all convolution kernels of the step (conv_fwd, conv_wgrad) "
                                    "plus their elementwise kernels", "peak_source": kind},
-            "cpu_baseline": None,
+            "cpu_baseline": cpu,
             "e2e": {"value": world * flops / t_e2e / 1e12, "unit": "TFLOP/s",
                     "h2d_bytes_per_step": int(x_h.nbytes + tf_h.nbytes + tp_h.nbytes),
                     "d2h_bytes_per_step": 4},

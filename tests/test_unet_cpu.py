@@ -149,3 +149,12 @@ def test_relu_mask_rule_matches_autograd():
             else:
                 got = gx[..., 0]
     np.testing.assert_allclose(got.numpy(), want.numpy(), rtol=1e-9, atol=1e-12)
+
+
+def test_bench_cpu_sample_of_the_unet():
+    """bench.py's CPU baseline of the unet workload: the oracle network's
+    training step on the host cores, a bounded sample."""
+    import bench
+
+    tflops, steps, seconds, threads = bench.cpu_sample_unet(target_s=0.5, batch=1)
+    assert steps >= 1 and seconds > 0 and threads >= 1 and 0 < tflops < 50
