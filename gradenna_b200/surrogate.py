@@ -1,4 +1,4 @@
-"""Learned design surrogate with the FDTD solver as judge.
+"""Learned design surrogate with the FDTD solver as verifier.
 
 A BF16 U-Net (gradenna_b200.unet) is trained on density -> field pairs that
 the batched 2D solver itself generates, and then proposes design updates
@@ -24,7 +24,7 @@ Pieces:
 
 * ``AntennaProblem`` - the problem (``AntennaProblem()`` = the 1 mm hero,
   ``AntennaProblem.coarse()`` = the same geometry at 3 mm for tests);
-* ``evaluate`` - the FDTD judge: radiated fractions, design-region Ez
+* ``evaluate`` - the FDTD verifier: radiated fractions, design-region Ez
   phasors and exact gradients of many designs, both runs batched;
 * ``random_densities`` / ``generate_dataset`` - seeded filtered/projected
   densities solved by the batched kernel;
@@ -166,7 +166,7 @@ class AntennaProblem:
         return radiated_fraction
 
 
-class _Judge:
+class _Verifier:
     """Cached plan and objective of a problem on a device (and, for the
     pulse drive, the time-domain adjoint plan)."""
 
@@ -208,13 +208,13 @@ def forward_batch(problem: AntennaProblem, rhos, *, device=None,
     pulse drive, the design cells' Ez histories for the time-domain
     adjoint)."""
     dev = _native.require_cuda(device)
-    plan, obj = _Judge.get(problem, dev)
+    plan, obj = _Verifier.get(problem, dev)
     rhos = torch.as_tensor(rhos, device=dev).to(torch.float64).reshape((-1,) + problem.design_shape)
     designs = [fa._full_eps_sigma(problem.grid, problem.design_sigma(rho), None,
                                   problem.design_region, dev) for rho in rhos]
     kws = [fa._forward_kwargs(plan, e, s) for e, s in designs]
     if problem.drive_kind == "pulse":
-        cells = _Judge.tplan(problem, dev).cells  # design-cell Ez histories
+        cells = _Verifier.tplan(problem, dev).cells  # design-cell Ez histories
         for kw in kws:
             kw["probe_ij"] = cells
     fwd = simulate_tm_batch(kws, tile_config=tile_config, device=dev)
@@ -231,12 +231,12 @@ def adjoint_batch(state: _Forward, which, *, tile_config: int | None = None) -> 
     frequency-domain adjoint for the CW drive, the time-domain adjoint of
     gradenna_b200.time_adjoint for the pulse drive)."""
     problem, dev = state.problem, state.dev
-    plan, obj = _Judge.get(problem, dev)
+    plan, obj = _Verifier.get(problem, dev)
     pulse = problem.drive_kind == "pulse"
     if pulse:
         from gradenna_b200 import time_adjoint as ta
 
-        tp = _Judge.tplan(problem, dev)
+        tp = _Verifier.tplan(problem, dev)
     which = list(which)
     kws, at = [], []
     for k in which:
@@ -279,7 +279,7 @@ def adjoint_batch(state: _Forward, which, *, tile_config: int | None = None) -> 
 
 def evaluate(problem: AntennaProblem, rhos, *, gradient: bool = True, device=None,
              tile_config: int | None = None):
-    """FDTD judge of designs ``rhos`` (B, H, W): (fraction (B,) float64,
+    """FDTD verification of designs ``rhos`` (B, H, W): (fraction (B,) float64,
     ez (B, H, W) complex128 design-region phasor, grads) with grads a list
     of d fraction / d rho (H, W) float64 per design (None without
     ``gradient``). Forward runs batched, then adjoint runs batched."""

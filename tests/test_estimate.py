@@ -6,9 +6,9 @@ of 2000 steps needs a few tens of MB forward, tens of GB for a naive
 reverse sweep and low single-digit GB checkpointed; strip psi storage is
 cheaper than full; DFT memory scales with frequencies and dtype; the
 default checkpoint count is round(sqrt(N)); the fit report keys and
-monotonicity. The B200 figures cover this library's runs: the survey's
-2D (1024^2, K = 4) and 3D (160 x 160 x 64, K = 11) workloads and the hero's
-time-domain adjoint fit one B200 with a wide margin.
+monotonicity. The B200 figures cover this library's runs: the benchmark's
+2D (1024^2, K = 4) and 3D patch (160 x 160 x 64, K = 11) workloads and the
+280 x 280 antenna's time-domain adjoint fit one B200 with a wide margin.
 """
 
 import numpy as np

@@ -1,6 +1,6 @@
-"""The reference README's own example (README.md:24-39, the survey's first
-configuration): a 140 x 140 grid at 2 mm, a 50 ohm port at (70, 55) driven
-by gaussian_pulse_for_band(2, 3 GHz) for 3500 steps, CPML 10, copper design
+"""The reference README's own example (README.md:24-39): a 140 x 140 grid
+at 2 mm, a 50 ohm port at (70, 55) driven by gaussian_pulse_for_band(2,
+3 GHz) for 3500 steps, CPML 10, copper design
 sigma_from_density(rho) on [44:96, 60:112], and the gradient of the negative
 radiated power at 2.45 GHz through the box (20, 120, 20, 120) with respect
 to rho = 0.5 (52 x 52): written with this library's surface

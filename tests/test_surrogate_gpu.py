@@ -2,7 +2,7 @@
 cells (AntennaProblem.coarse(): 96 x 96 grid, 32 x 32 design, 2400 steps):
 
 * the batched training-data generator labels every design with the same
-  radiated fraction as the FDTD judge evaluating it alone;
+  radiated fraction as the FDTD verifier evaluating it alone;
 * the U-Net trained by its own kernels on 1024 solver-labelled designs
   predicts the held-out log radiated fraction (R^2 >= 0.7);
 * what the trained network gains: with the same outer-iteration budget the

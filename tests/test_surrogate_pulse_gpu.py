@@ -1,7 +1,7 @@
 """GPU checks of the antenna problem under the reference's pulse drive
 (AntennaProblem(drive_kind="pulse"): gaussian_pulse_for_band(1.5, 3.5 GHz)
-at the port, export_viz.py:136-138), judged with the exact time-domain
-adjoint: the batched judge's gradient equals time_domain_gradient chained
+at the port, export_viz.py:136-138), verified with the exact time-domain
+adjoint: the batched verifier's gradient equals time_domain_gradient chained
 through sigma_from_density, and a few plain Adam iterations on it raise the
 radiated fraction."""
 
@@ -15,7 +15,7 @@ import torch
 pytestmark = pytest.mark.gpu
 
 
-def test_pulse_judge_gradient_and_plain_steps():
+def test_pulse_verifier_gradient_and_plain_steps():
     from gradenna_b200 import surrogate as S
     from gradenna_b200.fdtd2d import Port
     from gradenna_b200.monitors import poynting_box_monitors
