@@ -93,6 +93,19 @@ struct MonW {
 constexpr int MAXW = 16;  // per-tile monitor parts staged in shared memory
 constexpr int MAXF = 64;  // monitors whose offsets the fold stages in shared memory
 
+// Row-march work item (one warp): owned rows [i0, i0 + rows) and owned
+// columns [j0, j0 + owned_cols), its point entries [pb, pe) in MPt order and
+// its monitor parts [mb, me).
+struct MTask {
+  int i0, j0, rows, cls, pb, pe, mb, me;
+};
+
+// A row-march point entry: cell (i, j), point index m, tag = type (bits 0-2,
+// march::P_*) | 8 if the warp owns the cell (records are written by owners).
+struct MPt {
+  int i, j, m, tag;
+};
+
 template <typename T>
 struct Dev {
   int nx, ny, ld, npml, n_steps, n_freq, R, tiles_x;
@@ -123,6 +136,7 @@ struct Dev {
   const double2 *src_w, *mx_w, *my_w, *ph_e, *ph_h;
   T *out_probe, *out_v, *out_i;
   const int* step_base;
+  const MPt* mpts;  // row-march point entries (sorted by warp, then row, then type)
 };
 
 // Offset of field cell (i, j) in a padded plane.
@@ -307,6 +321,9 @@ __device__ void fill_coef(const Dev<T>& d, Coef<T, EH, EW>& k, int ie, int je, i
     k.c_e[cidx] = j >= 1 && j <= ny - 2;
   }
 }
+
+// The row-march kernel (defined in this namespace).
+#include "tm2d_march.cuh"
 
 template <typename T>
 __device__ __forceinline__ void ld16(T* dst, const T* src) {
@@ -753,11 +770,36 @@ __global__ void tm_dft_scale(C* a, long long count, double s) {
 
 struct Layout {
   Cfg cfg;
+  // Row march (tm_march) instead of shared-memory tiles (tm_tb): then a
+  // "tile" is one warp's strip segment, cfg.ti its owned rows and cfg.tj its
+  // owned columns.
+  bool march = false;
   int ld = 0, rows = 0, tiles_x = 0, tiles_y = 0, n_tiles = 0, R = 32, n_gen = 0, n_int = 0;
-  long long plane = 0, mon_cells = 0, n_mw = 0;
+  long long plane = 0, mon_cells = 0, n_mw = 0, n_mpts = 0;
   size_t state[2], ca, cb, psi[2], zero_end, tile_list, off[5], pts[5], mons, mw_off, mw, mring,
-      step, eacc, total;
+      step, eacc, tasks, mpts, total;
 };
+
+// The row march serves every run that does not record the energy each step
+// (those take one step per launch) and is not forced onto a tile shape;
+// GDN_TM_KERNEL=tile selects the shared-memory tile kernels instead.
+static bool use_march(const GdnTmParams* p, int force_cfg) {
+  if (p->record_energy || force_cfg >= 0) return false;
+  const char* env = getenv("GDN_TM_KERNEL");
+  return !(env && env[0] == 't');
+}
+
+// Owned rows per march segment: GDN_TM_SEG, else 16 (8..64).
+static int march_seg() {
+  const char* env = getenv("GDN_TM_SEG");
+  const int v = env ? atoi(env) : 16;
+  return std::min(std::max(v, 8), march::SIMAX);
+}
+
+template <typename T>
+static Cfg march_cfg() {
+  return Cfg{march::TB, march_seg(), march::owned_cols<T>(), march::WPB * 32};
+}
 
 // Tile shape: one step per launch when the energy is recorded, else the
 // largest TB=4 shape that still yields two CTAs per SM's worth of tiles.
@@ -816,7 +858,7 @@ static long long monitor_parts(const GdnTmParams* p, const GdnTmPoints* pts, con
 static bool tile_is_interior(const GdnTmParams* p, const Cfg& c, int ty, int tx) {
   const int m = p->npml;
   const int r0 = ty * c.ti - c.tb, r1 = (ty + 1) * c.ti + c.tb;
-  const int c0 = tx * c.tj - HJ, c1 = (tx + 1) * c.tj + HJ;
+  const int c0 = tx * c.tj - HJ, c1 = (tx + 1) * c.tj + HJ;  // march: HJ == march::HJ
   return r0 >= m + 1 && r1 - 1 <= p->nx - 2 - m && c0 >= m + 1 && c1 - 1 <= p->ny - 2 - m;
 }
 
@@ -824,7 +866,9 @@ static bool tile_is_interior(const GdnTmParams* p, const Cfg& c, int ty, int tx)
 static Layout make_layout(const GdnTmParams* p, const GdnTmPoints* pts, size_t esize,
                           int ring_steps = 0, int force_cfg = -1) {
   Layout L;
-  L.cfg = pick_cfg(p, esize, force_cfg);
+  L.march = use_march(p, force_cfg);
+  L.cfg = L.march ? (esize == sizeof(float) ? march_cfg<float>() : march_cfg<double>())
+                  : pick_cfg(p, esize, force_cfg);
   const Cfg& c = L.cfg;
   L.tiles_x = int(div_up(p->ny, c.tj));
   L.tiles_y = int(div_up(p->nx, c.ti));
@@ -860,9 +904,18 @@ static Layout make_layout(const GdnTmParams* p, const GdnTmPoints* pts, size_t e
   L.zero_end = cv.take<char>(0);
   L.tile_list = cv.take<int>(L.n_tiles);  // general tiles first, then interior
   const int counts[5] = {p->n_sources, p->n_ports, p->n_mx, p->n_my, p->n_probes};
-  for (int k = 0; k < 5; ++k) {
-    L.off[k] = cv.take<int>(L.n_tiles + 1);
-    L.pts[k] = cv.take<Pt>(4 * size_t(std::max(counts[k], 1)));
+  if (L.march) {
+    // A point lies in the extended range of at most two segments x two strips.
+    long long np = 0;
+    for (int k = 0; k < 5; ++k) np += counts[k];
+    L.n_mpts = 4 * np;
+    L.tasks = cv.take<MTask>(size_t(L.n_tiles));
+    L.mpts = cv.take<MPt>(size_t(std::max<long long>(L.n_mpts, 1)));
+  } else {
+    for (int k = 0; k < 5; ++k) {
+      L.off[k] = cv.take<int>(L.n_tiles + 1);
+      L.pts[k] = cv.take<Pt>(4 * size_t(std::max(counts[k], 1)));
+    }
   }
   L.mons = cv.take<MonD>(size_t(std::max(p->n_monitors, 3)));
   L.mw_off = cv.take<int>(L.n_tiles + 1);
@@ -1005,7 +1058,21 @@ struct Run {
   double* eacc = nullptr;
   int* step_base = nullptr;
   const int* tiles = nullptr;  // L.n_gen general tile ids, then L.n_int interior
+  // Row march: tasks in launch order (general first) and their tile ids.
+  std::vector<MTask> mtasks;
+  std::vector<int> mtask_tiles;
+  const MTask* tasks = nullptr;
 };
+
+template <typename T>
+static int prepare_tiles(const GdnTmParams* p, const GdnTmPoints* pts, char* ws, Run<T>& R,
+                         cudaStream_t stream);
+template <typename T>
+static int prepare_march(const GdnTmParams* p, const GdnTmPoints* pts, char* ws, Run<T>& R,
+                         cudaStream_t stream);
+template <typename T>
+static int prepare_common(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuffers* b,
+                          char* ws, Run<T>& R, cudaStream_t stream);
 
 template <typename T, int TB, int TI, int TJ, bool GEN>
 static size_t tb_smem() {
@@ -1051,6 +1118,12 @@ static int set_kernel_attributes() {
   if ((st = set_attr_cfg<T, 0>()) || (st = set_attr_cfg<T, 1>()) || (st = set_attr_cfg<T, 2>()) ||
       (st = set_attr_cfg<T, 3>()) || (st = set_attr_cfg<T, 4>()) || (st = set_attr_cfg<T, NCFG>()))
     return st;
+  GDN_TRY_CUDA(cudaFuncSetAttribute(march::tm_march<T, true, true>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    int(march::WPB * march::warp_smem<T, true, true>())));
+  GDN_TRY_CUDA(cudaFuncSetAttribute(march::tm_march<T, false, false>,
+                                    cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    int(march::WPB * march::warp_smem<T, false, false>())));
   done = true;
   return GDN_OK;
 }
@@ -1106,13 +1179,29 @@ static uint64_t launch_tb(const Run<T>& R, int sub0, int nsub, cudaStream_t s, c
     si = side;
   }
   uint64_t k = 0;
-  if (ng > 0) {
-    launch_which<T, true>(which, R, R.tiles, ng, sub0, nsub, s);
-    ++k;
-  }
-  if (ni > 0) {
-    launch_which<T, false>(which, R, R.tiles + ng, ni, sub0, nsub, si);
-    ++k;
+  if (R.L.march) {
+    constexpr int W = march::WPB;
+    if (ng > 0) {
+      march::tm_march<T, true, true><<<unsigned(div_up(ng, W)), W * 32,
+                                       W * march::warp_smem<T, true, true>(), s>>>(
+          R.d, R.tasks, ng, sub0, nsub);
+      ++k;
+    }
+    if (ni > 0) {
+      march::tm_march<T, false, false><<<unsigned(div_up(ni, W)), W * 32,
+                                         W * march::warp_smem<T, false, false>(), si>>>(
+          R.d, R.tasks + ng, ni, sub0, nsub);
+      ++k;
+    }
+  } else {
+    if (ng > 0) {
+      launch_which<T, true>(which, R, R.tiles, ng, sub0, nsub, s);
+      ++k;
+    }
+    if (ni > 0) {
+      launch_which<T, false>(which, R, R.tiles + ng, ni, sub0, nsub, si);
+      ++k;
+    }
   }
   if (si != s) {
     cudaEventRecord(join, side);
@@ -1226,6 +1315,18 @@ static int prepare(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuff
   d.step_base = R.step_base;
   R.eacc = reinterpret_cast<double*>(ws + L.eacc);
 
+  d.mpts = reinterpret_cast<const MPt*>(ws + L.mpts);
+  int st = L.march ? prepare_march(p, pts, ws, R, stream) : prepare_tiles(p, pts, ws, R, stream);
+  if (st) return st;
+  return prepare_common(p, pts, b, ws, R, stream);
+}
+
+// Tile kernels: per-tile point bins and the general/interior tile lists.
+template <typename T>
+static int prepare_tiles(const GdnTmParams* p, const GdnTmPoints* pts, char* ws, Run<T>& R,
+                         cudaStream_t stream) {
+  const Layout& L = R.L;
+  Dev<T>& d = R.d;
   // Point bins (with halo copies except for probes). Pageable copies are
   // staged before cudaMemcpyAsync returns, so the vectors may go away.
   const int counts[5] = {p->n_sources, p->n_ports, p->n_mx, p->n_my, p->n_probes};
@@ -1262,6 +1363,93 @@ static int prepare(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuff
                                  cudaMemcpyHostToDevice, stream));
     R.tiles = reinterpret_cast<const int*>(ws + L.tile_list);
   }
+  return GDN_OK;
+}
+
+// Row march: one task per (segment, strip), general tasks first; every
+// point's copies in each task whose extended range holds it, sorted by task,
+// row and type (the order a step applies them).
+template <typename T>
+static int prepare_march(const GdnTmParams* p, const GdnTmPoints* pts, char* ws, Run<T>& R,
+                         cudaStream_t stream) {
+  const Layout& L = R.L;
+  const Cfg& c = L.cfg;
+  const int SI = c.ti, OW = c.tj, TBm = march::TB, HJm = march::HJ;
+  const int SW = OW + 2 * HJm;  // strip width (32 * V)
+  std::vector<int> order;
+  order.reserve(L.n_tiles);
+  for (int pass = 0; pass < 2; ++pass)
+    for (int ty = 0; ty < L.tiles_y; ++ty)
+      for (int tx = 0; tx < L.tiles_x; ++tx)
+        if (tile_is_interior(p, c, ty, tx) == (pass == 1)) order.push_back(ty * L.tiles_x + tx);
+  std::vector<int> pos(L.n_tiles);
+  for (int k = 0; k < L.n_tiles; ++k) pos[order[k]] = k;
+  struct Rec {
+    int task;
+    MPt e;
+  };
+  std::vector<Rec> rec;
+  rec.reserve(size_t(L.n_mpts));
+  const int counts[5] = {p->n_mx, p->n_my, p->n_ports, p->n_sources, p->n_probes};
+  const int32_t* is[5] = {pts->mx_i, pts->my_i, pts->port_i, pts->src_i, pts->probe_i};
+  const int32_t* js[5] = {pts->mx_j, pts->my_j, pts->port_j, pts->src_j, pts->probe_j};
+  const int types[5] = {march::P_MX, march::P_MY, march::P_PORT, march::P_SRC, march::P_PROBE};
+  for (int k = 0; k < 5; ++k) {
+    for (int m = 0; m < counts[k]; ++m) {
+      const int i = is[k][m], j = js[k][m];
+      const int oty = i / SI, otx = j / OW;
+      for (int ty = std::max(0, oty - 1); ty <= std::min(L.tiles_y - 1, oty + 1); ++ty)
+        for (int tx = std::max(0, otx - 1); tx <= std::min(L.tiles_x - 1, otx + 1); ++tx) {
+          const bool own = ty == oty && tx == otx;
+          if (!own && types[k] == march::P_PROBE) continue;
+          const int r0 = ty * SI - TBm, r1 = (ty + 1) * SI + TBm;
+          const int c0 = tx * OW - HJm, c1 = c0 + SW;
+          if (i < r0 || i >= r1 || j < c0 || j >= c1) continue;
+          rec.push_back({pos[ty * L.tiles_x + tx], MPt{i, j, m, types[k] | (own ? 8 : 0)}});
+        }
+    }
+  }
+  if ((long long)rec.size() > std::max<long long>(L.n_mpts, 1))
+    GDN_BAD_ARG("internal: %zu point entries, layout sized for %lld", rec.size(), L.n_mpts);
+  std::stable_sort(rec.begin(), rec.end(), [](const Rec& a, const Rec& b) {
+    if (a.task != b.task) return a.task < b.task;
+    if (a.e.i != b.e.i) return a.e.i < b.e.i;
+    return (a.e.tag & 7) < (b.e.tag & 7);
+  });
+  std::vector<MPt> ent(rec.size());
+  std::vector<int> off(L.n_tiles + 1, 0);
+  for (size_t k = 0; k < rec.size(); ++k) {
+    ent[k] = rec[k].e;
+    off[rec[k].task + 1]++;
+  }
+  for (int t = 0; t < L.n_tiles; ++t) off[t + 1] += off[t];
+  R.mtask_tiles = order;
+  R.mtasks.assign(L.n_tiles, MTask{});
+  for (int k = 0; k < L.n_tiles; ++k) {
+    const int t = order[k], ty = t / L.tiles_x, tx = t - ty * L.tiles_x;
+    MTask& tk = R.mtasks[k];
+    tk.i0 = ty * SI;
+    tk.j0 = tx * OW;
+    tk.rows = std::min(SI, p->nx - tk.i0);
+    tk.cls = k < L.n_gen ? 1 : 0;
+    tk.pb = off[k];
+    tk.pe = off[k + 1];
+    tk.mb = tk.me = 0;  // filled by prepare_common from the monitor parts
+  }
+  if (!ent.empty())
+    GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.mpts, ent.data(), ent.size() * sizeof(MPt),
+                                 cudaMemcpyHostToDevice, stream));
+  R.tasks = reinterpret_cast<const MTask*>(ws + L.tasks);
+  return GDN_OK;
+}
+
+// Monitors, monitor parts, DFT output clears, state clears and ca/cb padding.
+template <typename T>
+static int prepare_common(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuffers* b,
+                          char* ws, Run<T>& R, cudaStream_t stream) {
+  const Layout& L = R.L;
+  Dev<T>& d = R.d;
+  const int nx = p->nx, ny = p->ny, N = p->n_steps;
 
   // Monitors (full grid when none are listed).
   const bool f64acc = p->dft_f64 != 0;
@@ -1316,6 +1504,15 @@ static int prepare(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuff
                                    cudaMemcpyHostToDevice, stream));
     d.mw_off = reinterpret_cast<const int*>(ws + L.mw_off);
     d.mw = reinterpret_cast<const MonW*>(ws + L.mw);
+    if (L.march) {
+      for (size_t k = 0; k < R.mtasks.size(); ++k) {
+        const int t = R.mtask_tiles[k];
+        R.mtasks[k].mb = moff[t];
+        R.mtasks[k].me = moff[t + 1];
+      }
+      GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.tasks, R.mtasks.data(), R.mtasks.size() * sizeof(MTask),
+                                   cudaMemcpyHostToDevice, stream));
+    }
   }
   R.max_cells = 0;
   for (const MonD& m : R.mons) {
@@ -1711,22 +1908,17 @@ constexpr size_t kStaticScratchBytes = size_t(32) << 20;  // 32 MiB per device
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticScratchBytes];
 
 // Device address of g_static_scratch on the current device. In host code the
-// array's name is only a host-side stand-in, so the address is looked up once
-// per device with cudaGetSymbolAddress (the first call on each device does
-// this set-up).
+// array's name is only a host-side stand-in, so every call looks the address
+// up with cudaGetSymbolAddress, with the caller's device current. The lookup
+// is cheap and allocates nothing once the module is loaded; doing it on every
+// call (instead of caching it) keeps the address right after a device reset,
+// which reloads the module elsewhere. With CUDA's lazy module loading, the
+// first lookup on a device loads this library's module, which reserves the
+// array itself (and the module's code) on that device.
 static int static_scratch(char** out) {
-  static std::mutex mu;
-  static char* addr[64] = {};
-  int dev = 0;
-  GDN_TRY_CUDA(cudaGetDevice(&dev));
-  if (dev < 0 || dev >= 64) GDN_BAD_ARG("device ordinal %d out of range", dev);
-  std::lock_guard<std::mutex> lock(mu);
-  if (!addr[dev]) {
-    void* p = nullptr;
-    GDN_TRY_CUDA(cudaGetSymbolAddress(&p, g_static_scratch));
-    addr[dev] = static_cast<char*>(p);
-  }
-  *out = addr[dev];
+  void* p = nullptr;
+  GDN_TRY_CUDA(cudaGetSymbolAddress(&p, g_static_scratch));
+  *out = static_cast<char*>(p);
   return GDN_OK;
 }
 
