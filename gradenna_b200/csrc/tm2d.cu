@@ -876,8 +876,11 @@ static Layout make_layout(const GdnTmParams* p, const GdnTmPoints* pts, size_t e
   L.ld = PADJ + L.tiles_x * c.tj + PADJ;
   L.rows = L.tiles_y * c.ti + 2 * PADI;
   L.plane = (long long)L.rows * L.ld;
-  L.mon_cells = pts ? monitor_cells(p, pts) : 0;
-  L.n_mw = pts ? monitor_parts(p, pts, c) : 0;
+  // Without a monitor list (n_monitors == 0) a DFT records the full grid;
+  // the points are only read for listed monitors, so pts may be NULL then.
+  const bool mons_known = pts || p->n_monitors == 0;
+  L.mon_cells = mons_known ? monitor_cells(p, pts) : 0;
+  L.n_mw = mons_known ? monitor_parts(p, pts, c) : 0;
   if (ring_steps > 0) {
     L.R = ring_steps;
   } else {

@@ -14,10 +14,11 @@
 //   * One launch advances TB = 4 time steps as a wavefront: at march step t
 //     row t is loaded and level s (time step n0 + s - 1) updates row t - s,
 //     so level s sees level s-1's new row below it and its own previous row
-//     above it. Every row in flight keeps its fields, coefficients and psi in
-//     a register slot (TB + 2 slots, the march loop unrolled over them), so
-//     each level updates its row in place; row t - TB leaves as a finished
-//     row after level TB.
+//     above it. Rows in flight sit in a register shift register: slot s holds
+//     row t - s, level s updates slot s in place, row t - TB leaves as a
+//     finished row after level TB, and the slots move down by one per step
+//     (register moves keep the loop body one step long, small enough for the
+//     instruction cache with many warps per SM).
 //   * Horizontal neighbours come from warp shuffles (Ez to the right for H,
 //     Hx to the left for E); vertical neighbours are the adjacent slots.
 //     Wrong values at the strip's outer lanes stay inside the halo: each
@@ -38,13 +39,13 @@
 namespace march {
 
 constexpr int TB = 4;         // time steps per launch (levels of the wavefront)
-constexpr int NSL = TB + 2;   // register row slots in flight
+constexpr int NSL = TB + 2;   // register row slots: rows t .. t - TB - 1
 constexpr int PF = 3;         // rows requested ahead of use
 constexpr int NST = PF + 2;   // cp.async ring stages per warp (one spare: no reuse hazard)
 constexpr int WPB = 4;        // warps per CTA
 constexpr int HJ = 4;         // halo columns per side (>= TB, a multiple of V)
 constexpr int SIMAX = 64;     // most owned rows per segment
-constexpr int MAXE = 128;     // point entries per warp whose values are staged
+constexpr int MAXE = 256;     // point entries per warp whose values are staged
 constexpr int MAXMW = 8;      // monitor parts per warp staged in shared memory
 
 // Point entry types, in the order a step processes them.
@@ -109,29 +110,34 @@ __device__ __forceinline__ T entry_value(const Dev<T>& d, const T* sval, int e, 
 
 // Point work of one row on the warp's row scratch `row` = [E^n | Hx | Hy |
 // Hy of the row above | E^{n+1}], 32*V columns each starting at column je.
-// Every lane walks the row's entries; the lane holding an entry's column
-// applies it, so repeated entries of a cell apply in list order. Returns the
-// end of the row's entries.
+// The row's entries are spread over the lanes; injections are shared-memory
+// atomic adds, so several entries on one cell all land. Returns the end of
+// the row's entries (they are a prefix of [q0, pe): the list is sorted by
+// row and q0 is the first entry of row r).
 template <typename T>
 __device__ __noinline__ int points_h(const Dev<T>& d, const MTask& tk, const T* sval, T* row,
                                      int je, int q0, int r, int s, int n) {
   constexpr int RW = 32 * Lanes<T>::V;
   const int lane = threadIdx.x & 31;
   int q1 = q0;
-  while (q1 < tk.pe && d.mpts[q1].i == r) ++q1;
-  for (int q = q0; q < q1; ++q) {  // Mx / My (fdtd2d.py:419-428)
+  for (;;) {
+    const int q = q1 + lane;
+    const unsigned in = __ballot_sync(0xffffffffu, q < tk.pe && d.mpts[q].i == r);
+    q1 += __popc(in);
+    if (in != 0xffffffffu) break;
+  }
+  for (int q = q0 + lane; q < q1; q += 32) {  // Mx / My (fdtd2d.py:419-428)
     const MPt p = d.mpts[q];
-    const int ty = p.tag & 7, o = p.j - je;
-    if ((ty == P_MX || ty == P_MY) && lane == o / Lanes<T>::V) {
-      const T v = entry_value(d, sval, q - tk.pb, ty, p.m, s, n);
-      row[(ty == P_MX ? RW : 2 * RW) + o] -= v;
-    }
+    const int ty = p.tag & 7;
+    if (ty == P_MX || ty == P_MY)
+      atomicAdd(row + (ty == P_MX ? RW : 2 * RW) + (p.j - je),
+                -entry_value(d, sval, q - tk.pb, ty, p.m, s, n));
   }
   __syncwarp();
-  for (int q = q0; q < q1; ++q) {  // port current on H^{n+1/2} (fdtd2d.py:430-436)
+  for (int q = q0 + lane; q < q1; q += 32) {  // port current on H^{n+1/2} (fdtd2d.py:430-436)
     const MPt p = d.mpts[q];
     const int o = p.j - je;
-    if ((p.tag & 7) == P_PORT && (p.tag & 8) && lane == o / Lanes<T>::V)
+    if ((p.tag & 7) == P_PORT && (p.tag & 8))
       d.out_i[(long long)n * d.n_ports + p.m] =
           (row[2 * RW + o] - row[3 * RW + o]) * d.dy - (row[RW + o] - row[RW + o - 1]) * d.dx;
   }
@@ -144,28 +150,24 @@ __device__ __noinline__ void points_e(const Dev<T>& d, const MTask& tk, const T*
   constexpr int RW = 32 * Lanes<T>::V;
   const int lane = threadIdx.x & 31;
   T* en = row + 4 * RW;
-  for (int q = q0; q < q1; ++q) {  // Jz (fdtd2d.py:444)
+  for (int q = q0 + lane; q < q1; q += 32) {  // Jz (fdtd2d.py:444)
     const MPt p = d.mpts[q];
-    const int o = p.j - je;
-    if ((p.tag & 7) == P_SRC && lane == o / Lanes<T>::V)
-      en[o] -= entry_value(d, sval, q - tk.pb, P_SRC, p.m, s, n);
+    if ((p.tag & 7) == P_SRC)
+      atomicAdd(en + (p.j - je), -entry_value(d, sval, q - tk.pb, P_SRC, p.m, s, n));
   }
-  for (int q = q0; q < q1; ++q) {  // RVS injection, every port (fdtd2d.py:446-448)
+  __syncwarp();
+  for (int q = q0 + lane; q < q1; q += 32) {  // RVS injection, every port (fdtd2d.py:446-448)
     const MPt p = d.mpts[q];
-    const int o = p.j - je;
-    if ((p.tag & 7) == P_PORT && lane == o / Lanes<T>::V)
-      en[o] += -entry_value(d, sval, q - tk.pb, P_PORT, p.m, s, n);
+    if ((p.tag & 7) == P_PORT)
+      atomicAdd(en + (p.j - je), -entry_value(d, sval, q - tk.pb, P_PORT, p.m, s, n));
   }
-  for (int q = q0; q < q1; ++q) {  // V = -dz (Ez^n + Ez^{n+1}) / 2 (fdtd2d.py:449-451)
+  __syncwarp();
+  for (int q = q0 + lane; q < q1; q += 32) {  // V (fdtd2d.py:449-451) and probes (:461)
     const MPt p = d.mpts[q];
-    const int o = p.j - je;
-    if ((p.tag & 7) == P_PORT && (p.tag & 8) && lane == o / Lanes<T>::V)
+    const int o = p.j - je, ty = p.tag & 7;
+    if (ty == P_PORT && (p.tag & 8))
       d.out_v[(long long)n * d.n_ports + p.m] = T(-0.5) * d.dz * (row[o] + en[o]);
-  }
-  for (int q = q0; q < q1; ++q) {  // probes (fdtd2d.py:461)
-    const MPt p = d.mpts[q];
-    const int o = p.j - je;
-    if ((p.tag & 7) == P_PROBE && lane == o / Lanes<T>::V)
+    else if (ty == P_PROBE)
       d.out_probe[(long long)n * d.n_probes + p.m] = en[o];
   }
 }
@@ -248,10 +250,12 @@ struct March {
     }
   }
 
-  // Level S (time step n0 + S - 1) on the row in slot Q; QD is the row
-  // below, QU the row above.
-  template <int S, int Q, int QD, int QU>
+  // Level S (time step n0 + S - 1) on the row in slot Q = S; the row below
+  // is in slot S - 1 (already at level S - 1), the row above in slot S + 1
+  // (at level S since the previous step).
+  template <int S>
   __device__ __forceinline__ void level(int r) {
+    constexpr int Q = S, QD = S - 1, QU = S + 1;
     const int s = S - 1;
     const int n = n0 + s;
     const T dt_mu = d.dt_mu, inv_dx = d.inv_dx, inv_dy = d.inv_dy;
@@ -408,27 +412,46 @@ struct March {
     }
   }
 
-  template <int S, int U>
-  __device__ __forceinline__ void level_if(int k, int t) {
-    if (S <= nsub && k >= S)
-      level<S, (U - S + NSL) % NSL, (U - S + 1 + NSL) % NSL, (U - S - 1 + 2 * NSL) % NSL>(t - S);
+  // Move every slot down by one row; the last slot keeps only Hy (the row
+  // above level TB).
+  __device__ __forceinline__ void shift() {
+#pragma unroll
+    for (int c = 0; c < V; ++c) HY[TB + 1][c] = HY[TB][c];
+#pragma unroll
+    for (int u = TB; u >= 1; --u)
+#pragma unroll
+      for (int c = 0; c < V; ++c) {
+        E[u][c] = E[u - 1][c];
+        HX[u][c] = HX[u - 1][c];
+        HY[u][c] = HY[u - 1][c];
+        CA[u][c] = CA[u - 1][c];
+        CB[u][c] = CB[u - 1][c];
+        if constexpr (XS) {
+          PEX[u][c] = PEX[u - 1][c];
+          PHY[u][c] = PHY[u - 1][c];
+        }
+        if constexpr (YS) {
+          PEY[u][c] = PEY[u - 1][c];
+          PHX[u][c] = PHX[u - 1][c];
+        }
+      }
   }
 
-  // March step k: row t = tstart + k enters slot U.
-  template <int U>
+  // March step k: row t = tstart + k enters slot 0.
   __device__ __forceinline__ void step(int k) {
     cp_async_wait<PF - 1>();
-    take<U>(k % NST);
+    take<0>(k % NST);
     if (k + PF < nsteps) issue(tstart + k + PF, (k + PF) % NST);
     cp_async_commit();
     const int t = tstart + k;
     static_assert(TB == 4, "levels are unrolled for TB = 4");
-    level_if<1, U>(k, t);
-    level_if<2, U>(k, t);
-    level_if<3, U>(k, t);
-    level_if<4, U>(k, t);
+    if (k >= 1 && nsub >= 1) level<1>(t - 1);
+    if (k >= 2 && nsub >= 2) level<2>(t - 2);
+    if (k >= 3 && nsub >= 3) level<3>(t - 3);
+    if (k >= 4 && nsub >= 4) level<4>(t - 4);
     const int r = t - TB;
-    if (k >= 2 * TB && r < tk.i0 + tk.rows && r < d.nx) store<(U - TB + NSL) % NSL>(r);
+    if (k >= 2 * TB && r < tk.i0 + tk.rows && r < d.nx) store<TB>(r);
+    shift();
   }
 };
 
@@ -551,15 +574,7 @@ __global__ void __launch_bounds__(WPB * 32) tm_march(const __grid_constant__ Dev
       if constexpr (YS) m.PEY[u][c] = m.PHX[u][c] = T(0);
     }
   __syncwarp();
-  static_assert(NSL == 6, "march steps are unrolled over 6 slots");
-  for (int k0 = 0; k0 < m.nsteps; k0 += NSL) {
-    m.template step<0>(k0);
-    if (k0 + 1 < m.nsteps) m.template step<1>(k0 + 1);
-    if (k0 + 2 < m.nsteps) m.template step<2>(k0 + 2);
-    if (k0 + 3 < m.nsteps) m.template step<3>(k0 + 3);
-    if (k0 + 4 < m.nsteps) m.template step<4>(k0 + 4);
-    if (k0 + 5 < m.nsteps) m.template step<5>(k0 + 5);
-  }
+  for (int k = 0; k < m.nsteps; ++k) m.step(k);
   cp_async_wait<0>();
 }
 

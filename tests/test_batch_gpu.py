@@ -2,8 +2,8 @@
 
 * A population of uneven problems (different grids, CPML thicknesses, step
   counts, sources, ports, DFT frequencies and monitor layouts) run as one
-  batch equals each problem run alone, bit for bit, under every tile
-  configuration; across configurations the probe, port and DFT records
+  batch equals each problem run alone with the same tile kernels, bit for
+  bit, under every tile configuration; across configurations the probe, port and DFT records
   agree to float32 rounding (2e-5 of their peak).
 * The batched frequency-domain adjoint gradient equals the one-problem
   gradient of each problem.
@@ -66,15 +66,17 @@ def _single(kw, cfg):
 
     kw = dict(kw)
     grid = kw.pop("grid")
-    old = os.environ.get("GDN_TM_TILE")
+    old = {k: os.environ.get(k) for k in ("GDN_TM_TILE", "GDN_TM_KERNEL")}
     os.environ["GDN_TM_TILE"] = str(cfg)
+    os.environ["GDN_TM_KERNEL"] = "tile"  # batches run the tile kernels
     try:
         return gb.simulate_tm(grid, **kw)
     finally:
-        if old is None:
-            del os.environ["GDN_TM_TILE"]
-        else:
-            os.environ["GDN_TM_TILE"] = old
+        for k, v in old.items():
+            if v is None:
+                del os.environ[k]
+            else:
+                os.environ[k] = v
 
 
 @pytest.mark.parametrize("cfg", [0, 1, 2, 3, 4])
@@ -116,8 +118,10 @@ def test_batch_rejects_unsupported():
     _ = gb
 
 
-def test_batched_adjoint_equals_single_gradients():
+def test_batched_adjoint_equals_single_gradients(monkeypatch):
     import gradenna_b200 as gb
+
+    monkeypatch.setenv("GDN_TM_KERNEL", "tile")  # the single runs use the batch's kernels
     from gradenna_b200.batch import freq_adjoint_gradient_batch
     from gradenna_b200.freq_adjoint import freq_adjoint_gradient
     from gradenna_b200.monitors import poynting_box_monitors, poynting_flux_box_2d
