@@ -212,11 +212,17 @@ int gdn_tm_run_batch_f32(const GdnTmProblem* problems, int32_t n, int32_t cfg, v
  * cudaMalloc/cudaFree, no graph instantiation (kernels are launched directly
  * on `stream`).
  *   - Runs whose scratch exceeds 32 MiB are rejected with GDN_ERR_BAD_ARG and
- *     a message giving the bytes needed (square grids up to about 830 x 830
- *     cells with a DFT, 960 x 960 without). The DFT fold length adapts to
- *     the capacity.
- *   - The first call on each device looks up the array's device address
- *     (cudaGetSymbolAddress); make that first call before any stream capture.
+ *     a message giving the bytes needed. With the default kernel settings
+ *     that is square grids up to about 670 x 670 cells without a DFT and
+ *     about 500 x 500 with a full-grid DFT (the DFT fold length shrinks to
+ *     fit; DFT monitor boxes cost ring space only for their own cells).
+ *   - Every call looks up the array's device address with
+ *     cudaGetSymbolAddress on the current device. The first call on a device
+ *     (or the first use of the library there, under CUDA's lazy module
+ *     loading) loads the library's module, which reserves the 32 MiB array
+ *     and the module's code on that device: make one warm-up call, before
+ *     any stream capture and before handing the rest of the GPU's memory to
+ *     a pool. After that a call allocates nothing.
  *   - All calls share the one array and it keeps the last call's contents;
  *     each call clears the state that must start at zero. Calls that overlap
  *     on the GPU (different streams, or other host threads) race on it and

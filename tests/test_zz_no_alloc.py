@@ -7,9 +7,11 @@ gdn_tm_run_noalloc_f32, which keeps its scratch in a fixed 32 MiB array
 inside the library. This test plays such a caller: it allocates every input
 and output once, up front, then calls the entry point through the C ABI
 twice in a row and checks both results against gdn_tm_run_f32 on the same
-inputs (the tolerance of the float32 parity tests: 1e-5 peak-normalised;
-in practice the results are identical). It also checks that an oversized
-run is refused with a clear error.
+inputs (the tolerance of the float32 parity tests: 1e-5 peak-normalised),
+and that the device's free memory does not move across the second call. A
+larger case with a full-grid DFT runs with a shortened monitor ring. The
+documented capacity is checked at its edges, and an oversized run is
+refused with a clear error.
 
 The file is named to run last, so a failing run with -x has already run
 every other test; it also passes on its own in a fresh process.
@@ -24,7 +26,7 @@ import torch
 pytestmark = pytest.mark.gpu
 
 
-def _case(dev):
+def _case(dev, nx=70, ny=53, n_steps=300):
     """A prepared 2D TM run: CPML, a Jz source, a driven port and a passive
     port, probes, a full-grid complex64 DFT at two frequencies."""
     from gradenna_b200 import _native
@@ -32,17 +34,17 @@ def _case(dev):
     from gradenna_b200.cpml import CPMLSpec, axis_coefficients, slab_tables
     from gradenna_b200.grid import Grid2D
 
-    g = Grid2D(70, 53, 2e-3, 2e-3)
-    nx, ny, npml, n_steps = g.nx, g.ny, 8, 300
+    g = Grid2D(nx, ny, 2e-3, 2e-3)
+    npml = 8
     dt = g.dt
     f32 = np.float32
     t = (np.arange(n_steps) + 0.5) * dt
     u = (t - 20 * dt) / (6 * dt)
     wave = (-u * np.exp(0.5 * (1.0 - u**2))).astype(f32)
-    src = np.array([[30, 21]], np.int32)
-    ports = np.array([[40, 30], [25, 35]], np.int32)
+    src = np.array([[3 * nx // 7, 2 * ny // 5]], np.int32)
+    ports = np.array([[4 * nx // 7, 4 * ny // 7], [5 * nx // 14, 2 * ny // 3]], np.int32)
     rs = np.array([50.0, 75.0])
-    probes = np.array([[10, 12], [50, 40], [0, 0]], np.int32)
+    probes = np.array([[nx // 7, ny // 4], [5 * nx // 7, 3 * ny // 4], [0, 0]], np.int32)
     freqs = np.array([3e9, 5e9])
 
     eps = np.full((nx, ny), EPS0, f32)
@@ -111,27 +113,45 @@ def _outputs(b, dims, dev):
         "dft_hx": torch.empty((2, nx, ny - 1), dtype=torch.complex64, device=dev),
         "dft_hy": torch.empty((2, nx - 1, ny), dtype=torch.complex64, device=dev),
     }
+    _bind(b, out)
+    return out
+
+
+def _bind(b, out):
+    """Point the buffer struct at one set of outputs (no allocation)."""
     b.ez, b.hx, b.hy = out["ez"].data_ptr(), out["hx"].data_ptr(), out["hy"].data_ptr()
     b.out_probe, b.out_v, b.out_i = out["probe"].data_ptr(), out["v"].data_ptr(), out["i"].data_ptr()
     b.dft_ez, b.dft_hx, b.dft_hy = (out[k].data_ptr() for k in ("dft_ez", "dft_hx", "dft_hy"))
-    return out
 
 
 def _rel(a, b):
     return float((a - b).abs().max() / (b.abs().max() + 1e-30))
 
 
-def test_noalloc_matches_regular_entry_point_twice():
-    from gradenna_b200 import _native
-
-    lib = _native.load()
+def _noalloc(lib):
     fn = lib.gdn_tm_run_noalloc_f32
     fn.restype = ctypes.c_int
-    fn.argtypes = [ctypes.POINTER(_native.TmParams), ctypes.POINTER(_native.TmPoints),
-                   ctypes.POINTER(_native.TmBuffers), ctypes.c_void_p]
+    fn.argtypes = [ctypes.POINTER(_native_mod().TmParams), ctypes.POINTER(_native_mod().TmPoints),
+                   ctypes.POINTER(_native_mod().TmBuffers), ctypes.c_void_p]
+    return fn
+
+
+def _native_mod():
+    from gradenna_b200 import _native
+
+    return _native
+
+
+def _compare_twice(nx, ny, n_steps):
+    """The regular entry point once, then the allocation-free one twice in a
+    row into separate outputs; every output of both calls must match, and
+    the second call must leave the device's free memory unchanged."""
+    _native = _native_mod()
+    lib = _native.load()
+    fn = _noalloc(lib)
     dev = torch.device("cuda", 0)
     torch.cuda.set_device(dev)
-    p, pts, b, _keep, dims = _case(dev)
+    p, pts, b, _keep, dims = _case(dev, nx, ny, n_steps)
     stream = ctypes.c_void_p(torch.cuda.current_stream(dev).cuda_stream)
 
     want = _outputs(b, dims, dev)
@@ -140,22 +160,61 @@ def test_noalloc_matches_regular_entry_point_twice():
     torch.cuda.synchronize()
     assert float(want["probe"].abs().max()) > 0.0
 
-    for _ in range(2):  # the second call must not see the first call's state
-        got = _outputs(b, dims, dev)
+    outs = [_outputs(b, dims, dev) for _ in range(2)]  # allocated before the calls
+    free = []
+    for got in outs:  # the second call must not see the first call's state
+        _bind(b, got)
+        torch.cuda.synchronize()
+        free.append(torch.cuda.mem_get_info(dev)[0])
         _native.check(fn(ctypes.byref(p), ctypes.byref(pts), ctypes.byref(b), stream))
         torch.cuda.synchronize()
         for k in want:
             assert _rel(got[k], want[k]) <= 1e-5, f"{k}: {_rel(got[k], want[k]):.2e}"
+    free.append(torch.cuda.mem_get_info(dev)[0])
+    # The first call may load the library's module on this device (lazy
+    # loading); from then on a call allocates nothing on the device.
+    assert free[2] == free[1], f"device free memory changed by {free[1] - free[2]} bytes"
+
+
+def test_noalloc_matches_regular_entry_point_twice():
+    _compare_twice(70, 53, 300)
+
+
+def test_noalloc_full_grid_dft_with_a_shortened_ring():
+    """At 420 x 420 with a full-grid DFT the monitor ring of 32 steps does not
+    fit the fixed scratch; the entry point shortens the ring (and folds the
+    DFT more often) and must still give the regular entry point's result."""
+    _compare_twice(420, 420, 120)
+
+
+def _status(nx, ny, dft):
+    _native = _native_mod()
+    lib = _native.load()
+    fn = _noalloc(lib)
+    dev = torch.device("cuda", 0)
+    p, pts, b, _keep, dims = _case(dev, nx, ny, 8)
+    _outputs(b, dims, dev)
+    if not dft:
+        p.n_freq = 0
+    st = fn(ctypes.byref(p), ctypes.byref(pts), ctypes.byref(b), None)
+    torch.cuda.synchronize()
+    return st, lib.gdn_last_error().decode()
+
+
+def test_noalloc_capacity_matches_the_documented_limits():
+    """The header states about 670 x 670 cells without a DFT and about
+    500 x 500 with a full-grid DFT (float32, default segment length)."""
+    assert _status(664, 664, dft=False)[0] == 0
+    assert _status(500, 500, dft=True)[0] == 0
+    for n, dft in ((704, False), (528, True)):
+        st, msg = _status(n, n, dft)
+        assert st == 1 and "static scratch" in msg, (n, dft, st, msg)
 
 
 def test_noalloc_rejects_runs_beyond_its_capacity():
-    from gradenna_b200 import _native
-
+    _native = _native_mod()
     lib = _native.load()
-    fn = lib.gdn_tm_run_noalloc_f32
-    fn.restype = ctypes.c_int
-    fn.argtypes = [ctypes.POINTER(_native.TmParams), ctypes.POINTER(_native.TmPoints),
-                   ctypes.POINTER(_native.TmBuffers), ctypes.c_void_p]
+    fn = _noalloc(lib)
     p, pts, b, _keep, dims = _case(torch.device("cuda", 0))
     _outputs(b, dims, torch.device("cuda", 0))
     p.nx = p.ny = 4096  # ~200 MiB of scratch; checked before any device work
