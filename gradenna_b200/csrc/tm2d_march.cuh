@@ -115,14 +115,14 @@ __device__ __forceinline__ T entry_value(const Dev<T>& d, const T* sval, int e, 
 // the row's entries (they are a prefix of [q0, pe): the list is sorted by
 // row and q0 is the first entry of row r).
 template <typename T>
-__device__ __noinline__ int points_h(const Dev<T>& d, const MTask& tk, const T* sval, T* row,
+__device__ __noinline__ int points_h(const Dev<T>& d, int pb, int pe, const T* sval, T* row,
                                      int je, int q0, int r, int s, int n) {
   constexpr int RW = 32 * Lanes<T>::V;
   const int lane = threadIdx.x & 31;
   int q1 = q0;
   for (;;) {
     const int q = q1 + lane;
-    const unsigned in = __ballot_sync(0xffffffffu, q < tk.pe && d.mpts[q].i == r);
+    const unsigned in = __ballot_sync(0xffffffffu, q < pe && d.mpts[q].i == r);
     q1 += __popc(in);
     if (in != 0xffffffffu) break;
   }
@@ -131,7 +131,7 @@ __device__ __noinline__ int points_h(const Dev<T>& d, const MTask& tk, const T* 
     const int ty = p.tag & 7;
     if (ty == P_MX || ty == P_MY)
       atomicAdd(row + (ty == P_MX ? RW : 2 * RW) + (p.j - je),
-                -entry_value(d, sval, q - tk.pb, ty, p.m, s, n));
+                -entry_value(d, sval, q - pb, ty, p.m, s, n));
   }
   __syncwarp();
   for (int q = q0 + lane; q < q1; q += 32) {  // port current on H^{n+1/2} (fdtd2d.py:430-436)
@@ -145,21 +145,21 @@ __device__ __noinline__ int points_h(const Dev<T>& d, const MTask& tk, const T* 
 }
 
 template <typename T>
-__device__ __noinline__ void points_e(const Dev<T>& d, const MTask& tk, const T* sval, T* row,
-                                      int je, int q0, int q1, int s, int n) {
+__device__ __noinline__ void points_e(const Dev<T>& d, int pb, const T* sval, T* row, int je,
+                                      int q0, int q1, int s, int n) {
   constexpr int RW = 32 * Lanes<T>::V;
   const int lane = threadIdx.x & 31;
   T* en = row + 4 * RW;
   for (int q = q0 + lane; q < q1; q += 32) {  // Jz (fdtd2d.py:444)
     const MPt p = d.mpts[q];
     if ((p.tag & 7) == P_SRC)
-      atomicAdd(en + (p.j - je), -entry_value(d, sval, q - tk.pb, P_SRC, p.m, s, n));
+      atomicAdd(en + (p.j - je), -entry_value(d, sval, q - pb, P_SRC, p.m, s, n));
   }
   __syncwarp();
   for (int q = q0 + lane; q < q1; q += 32) {  // RVS injection, every port (fdtd2d.py:446-448)
     const MPt p = d.mpts[q];
     if ((p.tag & 7) == P_PORT)
-      atomicAdd(en + (p.j - je), -entry_value(d, sval, q - tk.pb, P_PORT, p.m, s, n));
+      atomicAdd(en + (p.j - je), -entry_value(d, sval, q - pb, P_PORT, p.m, s, n));
   }
   __syncwarp();
   for (int q = q0 + lane; q < q1; q += 32) {  // V (fdtd2d.py:449-451) and probes (:461)
@@ -179,9 +179,17 @@ struct March {
   static constexpr int RW = 32 * V;  // elements of one plane row in a ring stage
   static constexpr bool GEN = XS || YS;
 
-  const Dev<T>& d;
-  const MTask& tk;
+  // Everything the march loop reads is held here by value (registers):
+  // reaching the kernel parameters or the task through a reference inside
+  // the loop costs a memory load per use.
+  const Dev<T>* dp;  // the kernel's parameter block (rare paths only)
   int lane, jl, tstart, nsteps, n0, nsub, par;
+  int nx, ld, rend, pb, pe, mb, R;
+  long long plane, mon_cells;
+  T dt_mu, inv_dx, inv_dy;
+  const T *src, *ca, *cb, *psrc;
+  T *dst, *pdst, *mring;
+  const MPt* mpts;
   T *ring, *sval, *rco, *prow;
   const MonW* smw;
   int nmw;
@@ -197,27 +205,25 @@ struct March {
   // Point cursors, one per level.
   int cur[TB + 1], nextrow[TB + 1];
 
-  __device__ __forceinline__ March(const Dev<T>& d_, const MTask& tk_) : d(d_), tk(tk_) {}
+  __device__ __forceinline__ March(const Dev<T>* d_) : dp(d_) {}
 
   __device__ __forceinline__ void issue(int i, int st) {
-    const long long g = cell_at(d.ld, i, jl);
-    const T* src = d.state[par];
+    const long long g = cell_at(ld, i, jl);
     T* s = ring + st * NPL * RW + lane * V;
     cp_async8(s, src + g);
-    cp_async8(s + RW, src + d.plane + g);
-    cp_async8(s + 2 * RW, src + 2 * d.plane + g);
-    cp_async8(s + 3 * RW, d.ca + g);
-    cp_async8(s + 4 * RW, d.cb + g);
-    const T* ps = d.psi[par];
+    cp_async8(s + RW, src + plane + g);
+    cp_async8(s + 2 * RW, src + 2 * plane + g);
+    cp_async8(s + 3 * RW, ca + g);
+    cp_async8(s + 4 * RW, cb + g);
     int p = 5;
     if constexpr (XS) {
-      cp_async8(s + p * RW, ps + g);                      // ezx
-      cp_async8(s + (p + 1) * RW, ps + 2 * d.plane + g);  // hyx
+      cp_async8(s + p * RW, psrc + g);                    // ezx
+      cp_async8(s + (p + 1) * RW, psrc + 2 * plane + g);  // hyx
       p += 2;
     }
     if constexpr (YS) {
-      cp_async8(s + p * RW, ps + d.plane + g);            // ezy
-      cp_async8(s + (p + 1) * RW, ps + 3 * d.plane + g);  // hxy
+      cp_async8(s + p * RW, psrc + plane + g);            // ezy
+      cp_async8(s + (p + 1) * RW, psrc + 3 * plane + g);  // hxy
     }
   }
 
@@ -258,7 +264,6 @@ struct March {
     constexpr int Q = S, QD = S - 1, QU = S + 1;
     const int s = S - 1;
     const int n = n0 + s;
-    const T dt_mu = d.dt_mu, inv_dx = d.inv_dx, inv_dy = d.inv_dy;
     T* e = E[Q];
     T* hx = HX[Q];
     T* hy = HY[Q];
@@ -270,9 +275,9 @@ struct March {
     if constexpr (XS) {
       const T* rc = rco + (r - tstart) * 8;
       rbh = rc[0]; rch = rc[1]; rkh = rc[2]; rbe = rc[3]; rce = rc[4]; rke = rc[5];
-      rHx = r >= 0 && r < d.nx;
-      rHy = r >= 0 && r < d.nx - 1;
-      rE = r >= 1 && r <= d.nx - 2;
+      rHx = r >= 0 && r < nx;
+      rHy = r >= 0 && r < nx - 1;
+      rE = r >= 1 && r <= nx - 2;
     }
     // ---- H (fdtd2d.py:416-428) ----
     const T e0r = __shfl_down_sync(0xffffffffu, e[0], 1);
@@ -315,7 +320,7 @@ struct March {
         prow[3 * RW + lane * V + c] = hyu[c];
       }
       __syncwarp();
-      pend = points_h<T>(d, tk, sval, prow, jl - lane * V, cur[S], r, s, n);
+      pend = points_h<T>(*dp, pb, pe, sval, prow, jl - lane * V, cur[S], r, s, n);
       __syncwarp();
 #pragma unroll
       for (int c = 0; c < V; ++c) {
@@ -349,18 +354,18 @@ struct March {
 #pragma unroll
       for (int c = 0; c < V; ++c) prow[4 * RW + lane * V + c] = e[c];
       __syncwarp();
-      points_e<T>(d, tk, sval, prow, jl - lane * V, cur[S], pend, s, n);
+      points_e<T>(*dp, pb, sval, prow, jl - lane * V, cur[S], pend, s, n);
       __syncwarp();
 #pragma unroll
       for (int c = 0; c < V; ++c) e[c] = prow[4 * RW + lane * V + c];
       cur[S] = pend;
-      nextrow[S] = pend < tk.pe ? d.mpts[pend].i : 0x7fffffff;
+      nextrow[S] = pend < pe ? mpts[pend].i : 0x7fffffff;
     }
     // ---- monitor ring (running DFT, fdtd2d.py:453-458) ----
     if (nmw > 0) {
-      T* slot = d.mring + (long long)(n % d.R) * d.mon_cells;
+      T* slot = mring + (long long)(n % R) * mon_cells;
       for (int q = 0; q < nmw; ++q) {
-        const MonW w = q < MAXMW ? smw[q] : d.mw[tk.mb + q];
+        const MonW w = q < MAXMW ? smw[q] : dp->mw[mb + q];
         if (r < w.a0 || r >= w.a1) continue;
         T* o = slot + w.base + (long long)r * w.w;
 #pragma unroll
@@ -375,22 +380,21 @@ struct March {
   // The finished row in slot Q (level TB) to the other state slot.
   template <int Q>
   __device__ __forceinline__ void store(int r) {
-    const long long g = cell_at(d.ld, r, jl);
-    T* dst = d.state[par ^ 1];
-    T* pd = d.psi[par ^ 1];
+    const long long g = cell_at(ld, r, jl);
+    T* pd = pdst;
     if constexpr (V == 2) {
       if (cown[0] && cown[1]) {
         using V2 = typename std::conditional<sizeof(T) == 4, float2, double2>::type;
         *reinterpret_cast<V2*>(dst + g) = V2{E[Q][0], E[Q][1]};
-        *reinterpret_cast<V2*>(dst + d.plane + g) = V2{HX[Q][0], HX[Q][1]};
-        *reinterpret_cast<V2*>(dst + 2 * d.plane + g) = V2{HY[Q][0], HY[Q][1]};
+        *reinterpret_cast<V2*>(dst + plane + g) = V2{HX[Q][0], HX[Q][1]};
+        *reinterpret_cast<V2*>(dst + 2 * plane + g) = V2{HY[Q][0], HY[Q][1]};
         if constexpr (XS) {
           *reinterpret_cast<V2*>(pd + g) = V2{PEX[Q][0], PEX[Q][1]};
-          *reinterpret_cast<V2*>(pd + 2 * d.plane + g) = V2{PHY[Q][0], PHY[Q][1]};
+          *reinterpret_cast<V2*>(pd + 2 * plane + g) = V2{PHY[Q][0], PHY[Q][1]};
         }
         if constexpr (YS) {
-          *reinterpret_cast<V2*>(pd + d.plane + g) = V2{PEY[Q][0], PEY[Q][1]};
-          *reinterpret_cast<V2*>(pd + 3 * d.plane + g) = V2{PHX[Q][0], PHX[Q][1]};
+          *reinterpret_cast<V2*>(pd + plane + g) = V2{PEY[Q][0], PEY[Q][1]};
+          *reinterpret_cast<V2*>(pd + 3 * plane + g) = V2{PHX[Q][0], PHX[Q][1]};
         }
         return;
       }
@@ -399,15 +403,15 @@ struct March {
     for (int c = 0; c < V; ++c) {
       if (!cown[c]) continue;
       dst[g + c] = E[Q][c];
-      dst[d.plane + g + c] = HX[Q][c];
-      dst[2 * d.plane + g + c] = HY[Q][c];
+      dst[plane + g + c] = HX[Q][c];
+      dst[2 * plane + g + c] = HY[Q][c];
       if constexpr (XS) {
         pd[g + c] = PEX[Q][c];
-        pd[2 * d.plane + g + c] = PHY[Q][c];
+        pd[2 * plane + g + c] = PHY[Q][c];
       }
       if constexpr (YS) {
-        pd[d.plane + g + c] = PEY[Q][c];
-        pd[3 * d.plane + g + c] = PHX[Q][c];
+        pd[plane + g + c] = PEY[Q][c];
+        pd[3 * plane + g + c] = PHX[Q][c];
       }
     }
   }
@@ -450,7 +454,7 @@ struct March {
     if (k >= 3 && nsub >= 3) level<3>(t - 3);
     if (k >= 4 && nsub >= 4) level<4>(t - 4);
     const int r = t - TB;
-    if (k >= 2 * TB && r < tk.i0 + tk.rows && r < d.nx) store<TB>(r);
+    if (k >= 2 * TB && r < rend) store<TB>(r);
     shift();
   }
 };
@@ -466,7 +470,7 @@ __global__ void __launch_bounds__(WPB * 32) tm_march(const __grid_constant__ Dev
   extern __shared__ __align__(16) unsigned char smem_raw[];
   unsigned char* wsm = smem_raw + size_t(warp) * warp_smem<T, XS, YS>();
   const MTask tk = tasks[tix];
-  March<T, XS, YS> m(d, tk);
+  March<T, XS, YS> m(&d);
   m.lane = threadIdx.x & 31;
   m.ring = reinterpret_cast<T*>(wsm);
   m.sval = m.ring + NST * planes<T, XS, YS>() * 32 * V;
@@ -480,6 +484,26 @@ __global__ void __launch_bounds__(WPB * 32) tm_march(const __grid_constant__ Dev
   m.jl = tk.j0 - HJ + m.lane * V;
   m.tstart = tk.i0 - TB;
   m.nsteps = tk.rows + 2 * TB;
+  m.nx = d.nx;
+  m.ld = d.ld;
+  m.rend = min(tk.i0 + tk.rows, d.nx);
+  m.pb = tk.pb;
+  m.pe = tk.pe;
+  m.mb = tk.mb;
+  m.R = d.R;
+  m.plane = d.plane;
+  m.mon_cells = d.mon_cells;
+  m.dt_mu = d.dt_mu;
+  m.inv_dx = d.inv_dx;
+  m.inv_dy = d.inv_dy;
+  m.src = d.state[m.par];
+  m.dst = d.state[m.par ^ 1];
+  m.ca = d.ca;
+  m.cb = d.cb;
+  m.psrc = d.psi[m.par];
+  m.pdst = d.psi[m.par ^ 1];
+  m.mring = d.mring;
+  m.mpts = d.mpts;
   const int lane = m.lane;
   // Start the ring first so the copies overlap the set-up below.
 #pragma unroll
