@@ -82,6 +82,7 @@ struct Dev3 {
   const Mon3* mons;
   const int* mw_off;  // per-CTA CSR over mw
   const MonW3* mw;
+  const unsigned char* cls;  // per plane-box work flags (F_*)
   T* cwv;                // CW source values of the chunk: [sub][cw_off[type] + m]
   long long cw_total, cw_off[6];
   const int* step_base;
@@ -170,70 +171,156 @@ __device__ __forceinline__ void write_monitors(const Dev3<T>& d, int c0, int c1,
   }
 }
 
+// Per plane-box flags (bit set = the box needs that work), computed on the
+// host so that most boxes run the bare stencil with no per-thread checks.
+enum : unsigned char { F_HPTS = 1, F_EPTS = 2, F_MON = 4, F_CPML = 8 };
+
+// Planes per CTA: a CTA walks NI consecutive i-planes of its (j, k) tile.
+constexpr int NI = 8;
+
+// H at one cell of plane i (fdtd3d.py:564-588), with (CP) or without the
+// CPML psi terms: boxes away from every slab skip the psi logic entirely.
+template <typename T, bool CP>
+__device__ __forceinline__ void h_cell(const Dev3<T>& d, int i, int j, int k, long long c) {
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  const T *ex = d.f[0], *ey = d.f[1], *ez = d.f[2];
+  T *hx = d.f[3], *hy = d.f[4], *hz = d.f[5];
+  const long long dj = d.sz, di = (long long)d.sy * d.sz;
+  const T e_c = ez[c], x_c = ex[c], y_c = ey[c];
+  // Hx (nx, ny-1, nz-1): +dt/mu (t_hxz - t_hxy)
+  if (j < ny - 1 && k < nz - 1) {
+    const T dey_dz = (ey[c + 1] - y_c) * d.inv_d[2];
+    const T dez_dy = (ez[c + dj] - e_c) * d.inv_d[1];
+    T tz = dey_dz, ty = dez_dy;
+    if constexpr (CP) {
+      tz = cpml<T, false>(d, 2, k, nz - 1, dey_dz, d.psi + P_HXZ * d.vol + c);
+      ty = cpml<T, false>(d, 1, j, ny - 1, dez_dy, d.psi + P_HXY * d.vol + c);
+    }
+    hx[c] = hx[c] + d.dt_mu * (tz - ty);
+  }
+  // Hy (nx-1, ny, nz-1): +dt/mu (t_hyx - t_hyz)
+  if (i < nx - 1 && k < nz - 1) {
+    const T dez_dx = (ez[c + di] - e_c) * d.inv_d[0];
+    const T dex_dz = (ex[c + 1] - x_c) * d.inv_d[2];
+    T tx = dez_dx, tz = dex_dz;
+    if constexpr (CP) {
+      tx = cpml<T, false>(d, 0, i, nx - 1, dez_dx, d.psi + P_HYX * d.vol + c);
+      tz = cpml<T, false>(d, 2, k, nz - 1, dex_dz, d.psi + P_HYZ * d.vol + c);
+    }
+    hy[c] = hy[c] + d.dt_mu * (tx - tz);
+  }
+  // Hz (nx-1, ny-1, nz): +dt/mu (t_hzy - t_hzx)
+  if (i < nx - 1 && j < ny - 1) {
+    const T dex_dy = (ex[c + dj] - x_c) * d.inv_d[1];
+    const T dey_dx = (ey[c + di] - y_c) * d.inv_d[0];
+    T ty = dex_dy, tx = dey_dx;
+    if constexpr (CP) {
+      ty = cpml<T, false>(d, 1, j, ny - 1, dex_dy, d.psi + P_HZY * d.vol + c);
+      tx = cpml<T, false>(d, 0, i, nx - 1, dey_dx, d.psi + P_HZX * d.vol + c);
+    }
+    hz[c] = hz[c] + d.dt_mu * (ty - tx);
+  }
+}
+
 // ---------------------------------------------------------------------------
 // H update: E^n -> H^{n+1/2} (fdtd3d.py:564-588) + Mx/My/Mz + H monitors.
+// A CTA covers a BJ x BK tile of NI consecutive i-planes.
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(NT) yee_h(Dev3<T> d, int sub) {
   const int n = *d.step_base + sub;
   const int k = blockIdx.x * BK + threadIdx.x;
   const int j = blockIdx.y * BJ + threadIdx.y;
-  const int i = blockIdx.z;
   const int nx = d.nx, ny = d.ny, nz = d.nz;
-  const T *ex = d.f[0], *ey = d.f[1], *ez = d.f[2];
-  T *hx = d.f[3], *hy = d.f[4], *hz = d.f[5];
-  if (j < ny && k < nz) {
-    const long long c = at(d, i, j, k);
-    const long long dj = d.sz, di = (long long)d.sy * d.sz;
-    // Hx (nx, ny-1, nz-1): +dt/mu (t_hxz - t_hxy)
-    if (j < ny - 1 && k < nz - 1) {
-      const T dey_dz = (ey[c + 1] - ey[c]) * d.inv_d[2];
-      const T dez_dy = (ez[c + dj] - ez[c]) * d.inv_d[1];
-      const T tz = cpml<T, false>(d, 2, k, nz - 1, dey_dz, d.psi + P_HXZ * d.vol + c);
-      const T ty = cpml<T, false>(d, 1, j, ny - 1, dez_dy, d.psi + P_HXY * d.vol + c);
-      hx[c] = hx[c] + d.dt_mu * (tz - ty);
-    }
-    // Hy (nx-1, ny, nz-1): +dt/mu (t_hyx - t_hyz)
-    if (i < nx - 1 && k < nz - 1) {
-      const T dez_dx = (ez[c + di] - ez[c]) * d.inv_d[0];
-      const T dex_dz = (ex[c + 1] - ex[c]) * d.inv_d[2];
-      const T tx = cpml<T, false>(d, 0, i, nx - 1, dez_dx, d.psi + P_HYX * d.vol + c);
-      const T tz = cpml<T, false>(d, 2, k, nz - 1, dex_dz, d.psi + P_HYZ * d.vol + c);
-      hy[c] = hy[c] + d.dt_mu * (tx - tz);
-    }
-    // Hz (nx-1, ny-1, nz): +dt/mu (t_hzy - t_hzx)
-    if (i < nx - 1 && j < ny - 1) {
-      const T dex_dy = (ex[c + dj] - ex[c]) * d.inv_d[1];
-      const T dey_dx = (ey[c + di] - ey[c]) * d.inv_d[0];
-      const T ty = cpml<T, false>(d, 1, j, ny - 1, dex_dy, d.psi + P_HZY * d.vol + c);
-      const T tx = cpml<T, false>(d, 0, i, nx - 1, dey_dx, d.psi + P_HZX * d.vol + c);
-      hz[c] = hz[c] + d.dt_mu * (ty - tx);
-    }
-  }
-  const int cta = (i * d.gj + blockIdx.y) * d.gk + blockIdx.x;
+  const bool live = j < ny && k < nz;
   const int tid = threadIdx.y * BK + threadIdx.x;
-  bool any = false;
-  for (int t = 3; t < 6; ++t) any |= d.off[t][cta] < d.off[t][cta + 1];
-  if (any) {
-    __syncthreads();
-    T* hs[3] = {hx, hy, hz};
-    for (int t = 3; t < 6; ++t) {
-      const int np_ = t == 3 ? d.n_mx : (t == 4 ? d.n_my : d.n_mz);
-      for (int q = d.off[t][cta] + tid; q < d.off[t][cta + 1]; q += NT) {
-        const Pt3 p = d.pts[t][q];
-        atomicAdd(hs[t - 3] + at(d, p.i, p.j, p.k), -(d.dt_mu * wave(d, t, np_, p.m, n, sub)));
+  const int i1 = min(nx, int(blockIdx.z + 1) * NI);
+  long long c = at(d, int(blockIdx.z) * NI, j, k);
+  const long long di = (long long)d.sy * d.sz;
+  for (int i = blockIdx.z * NI; i < i1; ++i, c += di) {
+    const int cta = (i * d.gj + blockIdx.y) * d.gk + blockIdx.x;
+    const unsigned fl = d.cls[cta];
+    if (live) {
+      if (fl & F_CPML)
+        h_cell<T, true>(d, i, j, k, c);
+      else
+        h_cell<T, false>(d, i, j, k, c);
+    }
+    if (fl & (F_HPTS | F_MON)) {
+      __syncthreads();
+      T* hs[3] = {d.f[3], d.f[4], d.f[5]};
+      if (fl & F_HPTS)
+        for (int t = 3; t < 6; ++t) {
+          const int np_ = t == 3 ? d.n_mx : (t == 4 ? d.n_my : d.n_mz);
+          for (int q = d.off[t][cta] + tid; q < d.off[t][cta + 1]; q += NT) {
+            const Pt3 p = d.pts[t][q];
+            atomicAdd(hs[t - 3] + at(d, p.i, p.j, p.k), -(d.dt_mu * wave(d, t, np_, p.m, n, sub)));
+          }
+        }
+      if (fl & F_MON) {
+        __syncthreads();
+        if (live) write_monitors(d, 3, 6, n, cta, i, j, k);
       }
     }
   }
-  if (d.n_mons > 0) {
-    __syncthreads();
-    if (j < ny && k < nz) write_monitors(d, 3, 6, n, cta, i, j, k);
+}
+
+// E at one cell of plane i (fdtd3d.py:596-626); for the port edge it also
+// leaves Ez^n, curl_z and the plain update in `s_port`.
+template <typename T, bool CP>
+__device__ __forceinline__ void e_cell(const Dev3<T>& d, int i, int j, int k, long long c,
+                                       bool port_here, T* s_port) {
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  T *ex = d.f[0], *ey = d.f[1], *ez = d.f[2];
+  const T *hx = d.f[3], *hy = d.f[4], *hz = d.f[5];
+  const long long dj = d.sz, di = (long long)d.sy * d.sz;
+  const long long g = ((long long)i * ny + j) * nz + k;  // node coefficients
+  const T hx_c = hx[c], hy_c = hy[c], hz_c = hz[c];
+  // Ex (nx-1, ny, nz) interior j, k: t_exy - t_exz
+  if (i < nx - 1 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2) {
+    const T dhz_dy = (hz_c - hz[c - dj]) * d.inv_d[1];
+    const T dhy_dz = (hy_c - hy[c - 1]) * d.inv_d[2];
+    T ty = dhz_dy, tz = dhy_dz;
+    if constexpr (CP) {
+      ty = cpml<T, true>(d, 1, j - 1, ny - 2, dhz_dy, d.psi + P_EXY * d.vol + c);
+      tz = cpml<T, true>(d, 2, k - 1, nz - 2, dhy_dz, d.psi + P_EXZ * d.vol + c);
+    }
+    ex[c] = d.ca[g] * ex[c] + d.cb[g] * (ty - tz);
+  }
+  // Ey (nx, ny-1, nz) interior i, k: t_eyz - t_eyx
+  if (i >= 1 && i <= nx - 2 && j < ny - 1 && k >= 1 && k <= nz - 2) {
+    const T dhx_dz = (hx_c - hx[c - 1]) * d.inv_d[2];
+    const T dhz_dx = (hz_c - hz[c - di]) * d.inv_d[0];
+    T tz = dhx_dz, tx = dhz_dx;
+    if constexpr (CP) {
+      tz = cpml<T, true>(d, 2, k - 1, nz - 2, dhx_dz, d.psi + P_EYZ * d.vol + c);
+      tx = cpml<T, true>(d, 0, i - 1, nx - 2, dhz_dx, d.psi + P_EYX * d.vol + c);
+    }
+    ey[c] = d.ca[g] * ey[c] + d.cb[g] * (tz - tx);
+  }
+  // Ez (nx, ny, nz-1) interior i, j: t_ezx - t_ezy
+  if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k < nz - 1) {
+    const T dhy_dx = (hy_c - hy[c - di]) * d.inv_d[0];
+    const T dhx_dy = (hx_c - hx[c - dj]) * d.inv_d[1];
+    T tx = dhy_dx, ty = dhx_dy;
+    if constexpr (CP) {
+      tx = cpml<T, true>(d, 0, i - 1, nx - 2, dhy_dx, d.psi + P_EZX * d.vol + c);
+      ty = cpml<T, true>(d, 1, j - 1, ny - 2, dhx_dy, d.psi + P_EZY * d.vol + c);
+    }
+    const T curl = tx - ty;
+    const T upd = d.ca[g] * ez[c] + d.cb[g] * curl;
+    if (port_here && i == d.pi && j == d.pj && k == d.pk) {
+      s_port[0] = ez[c];
+      s_port[1] = curl;
+      s_port[2] = upd;
+    }
+    ez[c] = upd;
   }
 }
 
 // ---------------------------------------------------------------------------
 // E update: H^{n+1/2} -> E^{n+1} (fdtd3d.py:596-633) + sources, port,
-// probes, V/I and E monitors.
+// probes, V/I and E monitors. Same CTA geometry as yee_h.
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(NT) yee_e(Dev3<T> d, int sub) {
@@ -241,85 +328,58 @@ __global__ void __launch_bounds__(NT) yee_e(Dev3<T> d, int sub) {
   const int n = *d.step_base + sub;
   const int k = blockIdx.x * BK + threadIdx.x;
   const int j = blockIdx.y * BJ + threadIdx.y;
-  const int i = blockIdx.z;
   const int nx = d.nx, ny = d.ny, nz = d.nz;
-  T *ex = d.f[0], *ey = d.f[1], *ez = d.f[2];
-  const T *hx = d.f[3], *hy = d.f[4], *hz = d.f[5];
-  const int cta = (i * d.gj + blockIdx.y) * d.gk + blockIdx.x;
-  const bool port_here = d.has_port && cta == d.port_cta;
-  if (j < ny && k < nz) {
-    const long long c = at(d, i, j, k);
-    const long long dj = d.sz, di = (long long)d.sy * d.sz;
-    const long long g = ((long long)i * ny + j) * nz + k;  // node coefficients
-    // Ex (nx-1, ny, nz) interior j, k: t_exy - t_exz
-    if (i < nx - 1 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2) {
-      const T dhz_dy = (hz[c] - hz[c - dj]) * d.inv_d[1];
-      const T dhy_dz = (hy[c] - hy[c - 1]) * d.inv_d[2];
-      const T ty = cpml<T, true>(d, 1, j - 1, ny - 2, dhz_dy, d.psi + P_EXY * d.vol + c);
-      const T tz = cpml<T, true>(d, 2, k - 1, nz - 2, dhy_dz, d.psi + P_EXZ * d.vol + c);
-      ex[c] = d.ca[g] * ex[c] + d.cb[g] * (ty - tz);
-    }
-    // Ey (nx, ny-1, nz) interior i, k: t_eyz - t_eyx
-    if (i >= 1 && i <= nx - 2 && j < ny - 1 && k >= 1 && k <= nz - 2) {
-      const T dhx_dz = (hx[c] - hx[c - 1]) * d.inv_d[2];
-      const T dhz_dx = (hz[c] - hz[c - di]) * d.inv_d[0];
-      const T tz = cpml<T, true>(d, 2, k - 1, nz - 2, dhx_dz, d.psi + P_EYZ * d.vol + c);
-      const T tx = cpml<T, true>(d, 0, i - 1, nx - 2, dhz_dx, d.psi + P_EYX * d.vol + c);
-      ey[c] = d.ca[g] * ey[c] + d.cb[g] * (tz - tx);
-    }
-    // Ez (nx, ny, nz-1) interior i, j: t_ezx - t_ezy
-    if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k < nz - 1) {
-      const T dhy_dx = (hy[c] - hy[c - di]) * d.inv_d[0];
-      const T dhx_dy = (hx[c] - hx[c - dj]) * d.inv_d[1];
-      const T tx = cpml<T, true>(d, 0, i - 1, nx - 2, dhy_dx, d.psi + P_EZX * d.vol + c);
-      const T ty = cpml<T, true>(d, 1, j - 1, ny - 2, dhx_dy, d.psi + P_EZY * d.vol + c);
-      const T curl = tx - ty;
-      const T upd = d.ca[g] * ez[c] + d.cb[g] * curl;
-      if (port_here && i == d.pi && j == d.pj && k == d.pk) {
-        s_port[0] = ez[c];
-        s_port[1] = curl;
-        s_port[2] = upd;
-      }
-      ez[c] = upd;
-    }
-  }
+  const bool live = j < ny && k < nz;
   const int tid = threadIdx.y * BK + threadIdx.x;
-  bool any = port_here;
-  for (int t = 0; t < 3; ++t) any |= d.off[t][cta] < d.off[t][cta + 1];
-  any |= d.off[6][cta] < d.off[6][cta + 1];
-  if (any) {
-    __syncthreads();
-    T* es[3] = {ez, ex, ey};  // point types 0 src (Jz), 1 jx, 2 jy
-    const T* cbs[3] = {d.cb_src, d.cb_jx, d.cb_jy};
-    const int nps[3] = {d.n_src, d.n_jx, d.n_jy};
-    for (int t = 0; t < 3; ++t)
-      for (int q = d.off[t][cta] + tid; q < d.off[t][cta + 1]; q += NT) {
-        const Pt3 p = d.pts[t][q];
-        atomicAdd(es[t] + at(d, p.i, p.j, p.k), -(cbs[t][p.m] * wave(d, t, nps[t], p.m, n, sub)));
+  const int i1 = min(nx, int(blockIdx.z + 1) * NI);
+  long long c = at(d, int(blockIdx.z) * NI, j, k);
+  const long long di = (long long)d.sy * d.sz;
+  for (int i = blockIdx.z * NI; i < i1; ++i, c += di) {
+    const int cta = (i * d.gj + blockIdx.y) * d.gk + blockIdx.x;
+    const unsigned fl = d.cls[cta];
+    const bool port_here = d.has_port && cta == d.port_cta;
+    if (live) {
+      if (fl & F_CPML)
+        e_cell<T, true>(d, i, j, k, c, port_here, s_port);
+      else
+        e_cell<T, false>(d, i, j, k, c, port_here, s_port);
+    }
+    if (fl & F_EPTS) {
+      T *ex = d.f[0], *ey = d.f[1], *ez = d.f[2];
+      const T *hx = d.f[3], *hy = d.f[4];
+      __syncthreads();
+      T* es[3] = {ez, ex, ey};  // point types 0 src (Jz), 1 jx, 2 jy
+      const T* cbs[3] = {d.cb_src, d.cb_jx, d.cb_jy};
+      const int nps[3] = {d.n_src, d.n_jx, d.n_jy};
+      for (int t = 0; t < 3; ++t)
+        for (int q = d.off[t][cta] + tid; q < d.off[t][cta + 1]; q += NT) {
+          const Pt3 p = d.pts[t][q];
+          atomicAdd(es[t] + at(d, p.i, p.j, p.k), -(cbs[t][p.m] * wave(d, t, nps[t], p.m, n, sub)));
+        }
+      __syncthreads();
+      if (port_here && tid == 0) {
+        const long long cp = at(d, d.pi, d.pj, d.pk);
+        // A current source on the port edge enters the port's semi-implicit
+        // update like the curl does: its plain increment (ez - upd, added by
+        // the source loop above) rescaled from c_b to the port's b.
+        const T src = ez[cp] - s_port[2];
+        const T ez_new = d.a_port * s_port[0] + d.b_port * s_port[1] + d.c_port * d.port_vs[n] +
+                         (src != T(0) ? src * (d.b_port / d.cb[((long long)d.pi * ny + d.pj) * nz + d.pk]) : T(0));
+        ez[cp] = ez_new;
+        d.out_v[n] = T(-0.5) * d.dz * (s_port[0] + ez_new);
+        const long long dj = d.sz;
+        d.out_i[n] = (hy[cp] - hy[cp - di]) * d.dy + (hx[cp - dj] - hx[cp]) * d.dx;
       }
-    __syncthreads();
-    if (port_here && tid == 0) {
-      const long long c = at(d, d.pi, d.pj, d.pk);
-      // A current source on the port edge enters the port's semi-implicit
-      // update like the curl does: its plain increment (ez - upd, added by
-      // the source loop above) rescaled from c_b to the port's b.
-      const T src = ez[c] - s_port[2];
-      const T ez_new = d.a_port * s_port[0] + d.b_port * s_port[1] + d.c_port * d.port_vs[n] +
-                       (src != T(0) ? src * (d.b_port / d.cb[((long long)d.pi * ny + d.pj) * nz + d.pk]) : T(0));
-      ez[c] = ez_new;
-      d.out_v[n] = T(-0.5) * d.dz * (s_port[0] + ez_new);
-      const long long dj = d.sz, di = (long long)d.sy * d.sz;
-      d.out_i[n] = (hy[c] - hy[c - di]) * d.dy + (hx[c - dj] - hx[c]) * d.dx;
+      __syncthreads();
+      for (int q = d.off[6][cta] + tid; q < d.off[6][cta + 1]; q += NT) {
+        const Pt3 p = d.pts[6][q];
+        d.out_probe[(long long)n * d.n_probes + p.m] = ez[at(d, p.i, p.j, p.k)];
+      }
     }
-    __syncthreads();
-    for (int q = d.off[6][cta] + tid; q < d.off[6][cta + 1]; q += NT) {
-      const Pt3 p = d.pts[6][q];
-      d.out_probe[(long long)n * d.n_probes + p.m] = ez[at(d, p.i, p.j, p.k)];
+    if (fl & F_MON) {
+      __syncthreads();
+      if (live) write_monitors(d, 0, 3, n, cta, i, j, k);
     }
-  }
-  if (d.n_mons > 0) {
-    __syncthreads();
-    if (j < ny && k < nz) write_monitors(d, 0, 3, n, cta, i, j, k);
   }
 }
 
@@ -498,7 +558,8 @@ static void comp_shape(int c, int nx, int ny, int nz, int s[3]) {
 struct Layout3 {
   int sy = 0, sz = 0, gj = 0, gk = 0, n_cta = 0, R = 32;
   long long vol = 0, mon_cells = 0, n_mw = 0;
-  size_t fields, psi, zero_end, off[7], pts[7], mons, mw_off, mw, mring, step, eacc, cwv, total;
+  size_t fields, psi, zero_end, off[7], pts[7], mons, mw_off, mw, mring, step, eacc, cwv, cls,
+      total;
 };
 
 // Monitor boxes {comp, lo0, lo1, lo2, s0, s1, s2} in ring order: the listed
@@ -591,6 +652,7 @@ static Layout3 make_layout3(const GdnYeeParams* p, const GdnYeePoints* pts, size
   if (p->cw_sources)
     for (int t = 0; t < 6; ++t) cw_total += count_of(p, t);
   L.cwv = cv.take<char>(size_t(std::max<long long>(cw_total * L.R, 1)) * esize);
+  L.cls = cv.take<unsigned char>(size_t(L.n_cta));
   L.total = cv.bytes();
   return L;
 }
@@ -812,6 +874,7 @@ static int run3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuff
     }
   }
   // Monitor parts per CTA (CSR over CTA ids (i * gj + j / BJ) * gk + k / BK).
+  std::vector<int> mon_off;
   {
     std::vector<int> cnt(L.n_cta + 1, 0);
     auto for_parts = [&](auto&& fn) {
@@ -842,6 +905,7 @@ static int run3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuff
     for_parts([&](int c, const MonW3& w) { mw[cur[c]++] = w; });
     GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.mw_off, cnt.data(), cnt.size() * sizeof(int),
                                  cudaMemcpyHostToDevice, stream));
+    mon_off = cnt;
     if (L.n_mw > 0)
       GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.mw, mw.data(), size_t(L.n_mw) * sizeof(MonW3),
                                    cudaMemcpyHostToDevice, stream));
@@ -850,6 +914,37 @@ static int run3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuff
   }
   d.n_mons = int(mons.size());
   d.mons = reinterpret_cast<const Mon3*>(ws + L.mons);
+  // Work flags per plane box: points of the H or E kernel (the port's box
+  // counts as E points), monitor parts, and any CPML slab within reach of
+  // the box (either field type, a margin of one cell).
+  {
+    std::vector<unsigned char> cls(L.n_cta, 0);
+    for (int t = 0; t < 7; ++t) {
+      const int n = count_of(p, t);
+      const int32_t* a = pts_of(pts, t);
+      for (int m = 0; m < n; ++m)
+        cls[(a[3 * m] * L.gj + a[3 * m + 1] / BJ) * L.gk + a[3 * m + 2] / BK] |=
+            (t >= 3 && t <= 5) ? F_HPTS : F_EPTS;
+    }
+    if (p->has_port) cls[d.port_cta] |= F_EPTS;
+    for (int c = 0; c < L.n_cta; ++c)
+      if (mon_off[c + 1] > mon_off[c]) cls[c] |= F_MON;
+    const int m = p->npml;
+    auto near_slab = [m](int lo, int hi, int n) {  // cells [lo, hi) of an axis of n nodes
+      return lo <= m + 1 || hi - 1 >= n - 2 - m;
+    };
+    for (int i = 0; i < nx; ++i)
+      for (int by = 0; by < L.gj; ++by)
+        for (int bx = 0; bx < L.gk; ++bx) {
+          const bool sl = m > 0 && (near_slab(i, i + 1, nx) ||
+                                    near_slab(by * BJ, std::min(ny, (by + 1) * BJ), ny) ||
+                                    near_slab(bx * BK, std::min(nz, (bx + 1) * BK), nz));
+          if (sl) cls[(i * L.gj + by) * L.gk + bx] |= F_CPML;
+        }
+    GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.cls, cls.data(), cls.size(), cudaMemcpyHostToDevice,
+                                 stream));
+    d.cls = reinterpret_cast<const unsigned char*>(ws + L.cls);
+  }
   long long max_cells = 0;
   for (const Mon3& m : mons) {
     max_cells = std::max(max_cells, m.count);
@@ -864,7 +959,7 @@ static int run3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuff
     GDN_TRY_CUDA(cudaMemsetAsync(eacc, 0, 2 * size_t(std::max(N, 1)) * sizeof(double), stream));
 
   const dim3 blk(BK, BJ);
-  const dim3 grd(L.gk, L.gj, nx);
+  const dim3 grd(L.gk, L.gj, unsigned(div_up(nx, NI)));
   const int eblocks = int(std::min<long long>(div_up((long long)nx * ny * nz, 256), 148 * 8));
   auto enqueue = [&](int cnt, cudaStream_t s) -> uint64_t {
     uint64_t k = 0;
