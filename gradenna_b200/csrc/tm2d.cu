@@ -265,6 +265,10 @@ struct Coef {
   T rb_h[EH], rc_h[EH], rk_h[EH], rb_e[EH], rc_e[EH], rk_e[EH];  // hyx, ezx (by row)
   T cb_h[EW], cc_h[EW], ck_h[EW], cb_e[EW], cc_e[EW], ck_e[EW];  // hxy, ezy (by column)
   unsigned char r_hx[EH], r_hy[EH], r_e[EH], c_hx[EW], c_hy[EW], c_e[EW];
+  // psi in use: rows inside an x slab (hyx, ezx) and 16-byte column groups
+  // touching a y slab (hxy, ezy). Elsewhere the psi recursion is identically
+  // zero (b = c = 0, 1/kappa = 1) and the sweeps skip it.
+  unsigned char x_h[EH], x_e[EH], y_h[EW / (16 / sizeof(T))], y_e[EW / (16 / sizeof(T))];
 };
 
 template <typename T, int EH, int EW, int NT>
@@ -294,6 +298,19 @@ __device__ void fill_coef(const Dev<T>& d, Coef<T, EH, EW>& k, int ie, int je, i
     k.r_hx[r] = i >= 0 && i < nx;
     k.r_hy[r] = i >= 0 && i < nx - 1;
     k.r_e[r] = i >= 1 && i <= nx - 2;
+    k.x_h[r] = i >= 0 && i < nx - 1 && (i < m || i >= nx - 1 - m);
+    k.x_e[r] = a >= 0 && a < ni && (a < m || a >= ni - m);
+  }
+  constexpr int V = 16 / sizeof(T);
+  for (int g = tid; g < EW / V; g += NT) {
+    bool h = false, e = false;
+    for (int u = 0; u < V; ++u) {
+      const int j = je + g * V + u, bb = j - 1;
+      h = h || (j >= 0 && j < ny - 1 && (j < m || j >= ny - 1 - m));
+      e = e || (bb >= 0 && bb < ny - 2 && (bb < m || bb >= ny - 2 - m));
+    }
+    k.y_h[g] = h;
+    k.y_e[g] = e;
   }
   for (int cidx = tid; cidx < EW; cidx += NT) {
     const int j = je + cidx;
@@ -427,24 +444,31 @@ __device__ __forceinline__ void tb_body(const Dev<T>& d, const int tile, int sub
       ld16(hy, sHy + q);
       if constexpr (GEN) {
         const int r = q / EW, c = q - r * EW;
+        const bool sy = K.y_h[c / V], sx = K.x_h[r];
         T pxy[V], pyx[V];
-        ld16(pxy, sPsi + 3 * EC + q);
-        ld16(pyx, sPsi + 2 * EC + q);
+        if (sy) ld16(pxy, sPsi + 3 * EC + q);
+        if (sx) ld16(pyx, sPsi + 2 * EC + q);
         const T rb = K.rb_h[r], rc = K.rc_h[r], rk = K.rk_h[r];
         const bool rhx = K.r_hx[r], rhy = K.r_hy[r];
 #pragma unroll
         for (int k = 0; k < V; ++k) {
           const T dy_ = (e[k + 1] - e[k]) * inv_dy;
-          pxy[k] = K.cb_h[c + k] * pxy[k] + K.cc_h[c + k] * dy_;
-          const T thx = dy_ * K.ck_h[c + k] + pxy[k];
+          T thx = dy_;
+          if (sy) {
+            pxy[k] = K.cb_h[c + k] * pxy[k] + K.cc_h[c + k] * dy_;
+            thx = dy_ * K.ck_h[c + k] + pxy[k];
+          }
           if (rhx && K.c_hx[c + k]) hx[k] -= dt_mu * thx;
           const T dx_ = (el[k] - e[k]) * inv_dx;
-          pyx[k] = rb * pyx[k] + rc * dx_;
-          const T thy = dx_ * rk + pyx[k];
+          T thy = dx_;
+          if (sx) {
+            pyx[k] = rb * pyx[k] + rc * dx_;
+            thy = dx_ * rk + pyx[k];
+          }
           if (rhy && K.c_hy[c + k]) hy[k] += dt_mu * thy;
         }
-        st16(sPsi + 3 * EC + q, pxy);
-        st16(sPsi + 2 * EC + q, pyx);
+        if (sy) st16(sPsi + 3 * EC + q, pxy);
+        if (sx) st16(sPsi + 2 * EC + q, pyx);
       } else {
 #pragma unroll
         for (int k = 0; k < V; ++k) {
@@ -486,23 +510,29 @@ __device__ __forceinline__ void tb_body(const Dev<T>& d, const int tile, int sub
       ld16(hu, sHy + (q >= EW ? q - EW : q));
       if constexpr (GEN) {
         const int r = q / EW, c = q - r * EW;
+        const bool sx = K.x_e[r], sy = K.y_e[c / V];
         T px[V], py[V];
-        ld16(px, sPsi + q);
-        ld16(py, sPsi + EC + q);
+        if (sx) ld16(px, sPsi + q);
+        if (sy) ld16(py, sPsi + EC + q);
         const T rb = K.rb_e[r], rc = K.rc_e[r], rk = K.rk_e[r];
         const bool re = K.r_e[r];
 #pragma unroll
         for (int k = 0; k < V; ++k) {
           const T dhy_dx = (hy[k] - hu[k]) * inv_dx;
           const T dhx_dy = (hx[k + 1] - hx[k]) * inv_dy;
-          px[k] = rb * px[k] + rc * dhy_dx;
-          py[k] = K.cb_e[c + k] * py[k] + K.cc_e[c + k] * dhx_dy;
-          const T tx_ = dhy_dx * rk + px[k];
-          const T ty_ = dhx_dy * K.ck_e[c + k] + py[k];
+          T tx_ = dhy_dx, ty_ = dhx_dy;
+          if (sx) {
+            px[k] = rb * px[k] + rc * dhy_dx;
+            tx_ = dhy_dx * rk + px[k];
+          }
+          if (sy) {
+            py[k] = K.cb_e[c + k] * py[k] + K.cc_e[c + k] * dhx_dy;
+            ty_ = dhx_dy * K.ck_e[c + k] + py[k];
+          }
           if (re && K.c_e[c + k]) e[k] = ca[k] * e[k] + cb[k] * (tx_ - ty_);
         }
-        st16(sPsi + q, px);
-        st16(sPsi + EC + q, py);
+        if (sx) st16(sPsi + q, px);
+        if (sy) st16(sPsi + EC + q, py);
       } else {
 #pragma unroll
         for (int k = 0; k < V; ++k)
