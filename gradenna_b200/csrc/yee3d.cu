@@ -178,48 +178,46 @@ enum : unsigned char { F_HPTS = 1, F_EPTS = 2, F_MON = 4, F_CPML = 8 };
 // Planes per CTA: a CTA walks NI consecutive i-planes of its (j, k) tile.
 constexpr int NI = 8;
 
-// H at one cell of plane i (fdtd3d.py:564-588), with (CP) or without the
-// CPML psi terms: boxes away from every slab skip the psi logic entirely.
-template <typename T, bool CP>
-__device__ __forceinline__ void h_cell(const Dev3<T>& d, int i, int j, int k, long long c) {
-  const int nx = d.nx, ny = d.ny, nz = d.nz;
-  const T *ex = d.f[0], *ey = d.f[1], *ez = d.f[2];
-  T *hx = d.f[3], *hy = d.f[4], *hz = d.f[5];
-  const long long dj = d.sz, di = (long long)d.sy * d.sz;
-  const T e_c = ez[c], x_c = ex[c], y_c = ey[c];
-  // Hx (nx, ny-1, nz-1): +dt/mu (t_hxz - t_hxy)
-  if (j < ny - 1 && k < nz - 1) {
-    const T dey_dz = (ey[c + 1] - y_c) * d.inv_d[2];
-    const T dez_dy = (ez[c + dj] - e_c) * d.inv_d[1];
-    T tz = dey_dz, ty = dez_dy;
-    if constexpr (CP) {
-      tz = cpml<T, false>(d, 2, k, nz - 1, dey_dz, d.psi + P_HXZ * d.vol + c);
-      ty = cpml<T, false>(d, 1, j, ny - 1, dez_dy, d.psi + P_HXY * d.vol + c);
-    }
-    hx[c] = hx[c] + d.dt_mu * (tz - ty);
+// CPML coefficients of sample s of axis ax (E-type: the ns = n-2 samples
+// of the PEC interior; H-type: the ns = n-1 half samples). Returns whether
+// s lies in a slab; outside, b = c = 0 and 1/kappa = 1 (cpml.py:161-208).
+template <typename T, bool E>
+__device__ __forceinline__ bool slab_coef(const Dev3<T>& d, int ax, int s, int ns, T& b, T& c,
+                                          T& ik) {
+  const int m = d.npml;
+  b = T(0);
+  c = T(0);
+  ik = T(1);
+  if (s < 0 || s >= ns) return false;
+  if (s < m) {
+    b = E ? d.be_lo[ax][s] : d.bh_lo[ax][s];
+    c = E ? d.ce_lo[ax][s] : d.ch_lo[ax][s];
+    ik = E ? d.ik_e[ax][s] : d.ik_h[ax][s];
+    return true;
   }
-  // Hy (nx-1, ny, nz-1): +dt/mu (t_hyx - t_hyz)
-  if (i < nx - 1 && k < nz - 1) {
-    const T dez_dx = (ez[c + di] - e_c) * d.inv_d[0];
-    const T dex_dz = (ex[c + 1] - x_c) * d.inv_d[2];
-    T tx = dez_dx, tz = dex_dz;
-    if constexpr (CP) {
-      tx = cpml<T, false>(d, 0, i, nx - 1, dez_dx, d.psi + P_HYX * d.vol + c);
-      tz = cpml<T, false>(d, 2, k, nz - 1, dex_dz, d.psi + P_HYZ * d.vol + c);
-    }
-    hy[c] = hy[c] + d.dt_mu * (tx - tz);
+  if (s >= ns - m) {
+    const int t = s - (ns - m);
+    b = E ? d.be_hi[ax][t] : d.bh_hi[ax][t];
+    c = E ? d.ce_hi[ax][t] : d.ch_hi[ax][t];
+    ik = E ? d.ik_e[ax][s] : d.ik_h[ax][s];
+    return true;
   }
-  // Hz (nx-1, ny-1, nz): +dt/mu (t_hzy - t_hzx)
-  if (i < nx - 1 && j < ny - 1) {
-    const T dex_dy = (ex[c + dj] - x_c) * d.inv_d[1];
-    const T dey_dx = (ey[c + di] - y_c) * d.inv_d[0];
-    T ty = dex_dy, tx = dey_dx;
-    if constexpr (CP) {
-      ty = cpml<T, false>(d, 1, j, ny - 1, dex_dy, d.psi + P_HZY * d.vol + c);
-      tx = cpml<T, false>(d, 0, i, nx - 1, dey_dx, d.psi + P_HZX * d.vol + c);
-    }
-    hz[c] = hz[c] + d.dt_mu * (ty - tx);
-  }
+  return false;
+}
+
+// One axis' CPML state of a thread: whether its sample is in a slab and the
+// coefficients there.
+template <typename T>
+struct Ax {
+  bool on;
+  T b, c, ik;
+};
+
+// psi <- b psi + c diff; the term diff/kappa + psi (cpml.py:120-158).
+template <typename T>
+__device__ __forceinline__ T psi_term(const Ax<T>& a, T diff, T& psi) {
+  psi = a.b * psi + a.c * diff;
+  return diff * a.ik + psi;
 }
 
 // ---------------------------------------------------------------------------
@@ -236,25 +234,84 @@ __global__ void __launch_bounds__(NT) yee_h(Dev3<T> d, int sub) {
   const int tid = threadIdx.y * BK + threadIdx.x;
   const int i1 = min(nx, int(blockIdx.z + 1) * NI);
   long long c = at(d, int(blockIdx.z) * NI, j, k);
-  const long long di = (long long)d.sy * d.sz;
+  const long long di = (long long)d.sy * d.sz, dj = d.sz, vol = d.vol;
+  const T *ex = d.f[0], *ey = d.f[1], *ez = d.f[2];
+  T *hx = d.f[3], *hy = d.f[4], *hz = d.f[5];
+  T* P = d.psi;
+  const T dt_mu = d.dt_mu, idx = d.inv_d[0], idy = d.inv_d[1], idz = d.inv_d[2];
+  // This thread's y and z CPML samples (H-type) are fixed over the planes.
+  Ax<T> ay, az;
+  ay.on = slab_coef<T, false>(d, 1, j, ny - 1, ay.b, ay.c, ay.ik);
+  az.on = slab_coef<T, false>(d, 2, k, nz - 1, az.b, az.c, az.ik);
   for (int i = blockIdx.z * NI; i < i1; ++i, c += di) {
     const int cta = (i * d.gj + blockIdx.y) * d.gk + blockIdx.x;
     const unsigned fl = d.cls[cta];
     if (live) {
-      if (fl & F_CPML)
-        h_cell<T, true>(d, i, j, k, c);
-      else
-        h_cell<T, false>(d, i, j, k, c);
+      Ax<T> ax;
+      ax.on = slab_coef<T, false>(d, 0, i, nx - 1, ax.b, ax.c, ax.ik);
+      // Every operand first (all in the padded volumes), then the updates.
+      const T ex0 = ex[c], ey0 = ey[c], ez0 = ez[c];
+      const T eyk = ey[c + 1], ezj = ez[c + dj], ezi = ez[c + di];
+      const T exk = ex[c + 1], exj = ex[c + dj], eyi = ey[c + di];
+      const T hx0 = hx[c], hy0 = hy[c], hz0 = hz[c];
+      const bool vx = j < ny - 1 && k < nz - 1, vy = i < nx - 1 && k < nz - 1,
+                 vz = i < nx - 1 && j < ny - 1;
+      T p_xz = T(0), p_xy = T(0), p_yx = T(0), p_yz = T(0), p_zy = T(0), p_zx = T(0);
+      if (vx && az.on) p_xz = P[P_HXZ * vol + c];
+      if (vx && ay.on) p_xy = P[P_HXY * vol + c];
+      if (vy && ax.on) p_yx = P[P_HYX * vol + c];
+      if (vy && az.on) p_yz = P[P_HYZ * vol + c];
+      if (vz && ay.on) p_zy = P[P_HZY * vol + c];
+      if (vz && ax.on) p_zx = P[P_HZX * vol + c];
+      if (vx) {  // Hx (nx, ny-1, nz-1): +dt/mu (t_hxz - t_hxy)
+        const T dey_dz = (eyk - ey0) * idz, dez_dy = (ezj - ez0) * idy;
+        T tz = dey_dz, ty = dez_dy;
+        if (az.on) {
+          tz = psi_term(az, dey_dz, p_xz);
+          P[P_HXZ * vol + c] = p_xz;
+        }
+        if (ay.on) {
+          ty = psi_term(ay, dez_dy, p_xy);
+          P[P_HXY * vol + c] = p_xy;
+        }
+        hx[c] = hx0 + dt_mu * (tz - ty);
+      }
+      if (vy) {  // Hy (nx-1, ny, nz-1): +dt/mu (t_hyx - t_hyz)
+        const T dez_dx = (ezi - ez0) * idx, dex_dz = (exk - ex0) * idz;
+        T tx = dez_dx, tz = dex_dz;
+        if (ax.on) {
+          tx = psi_term(ax, dez_dx, p_yx);
+          P[P_HYX * vol + c] = p_yx;
+        }
+        if (az.on) {
+          tz = psi_term(az, dex_dz, p_yz);
+          P[P_HYZ * vol + c] = p_yz;
+        }
+        hy[c] = hy0 + dt_mu * (tx - tz);
+      }
+      if (vz) {  // Hz (nx-1, ny-1, nz): +dt/mu (t_hzy - t_hzx)
+        const T dex_dy = (exj - ex0) * idy, dey_dx = (eyi - ey0) * idx;
+        T ty = dex_dy, tx = dey_dx;
+        if (ay.on) {
+          ty = psi_term(ay, dex_dy, p_zy);
+          P[P_HZY * vol + c] = p_zy;
+        }
+        if (ax.on) {
+          tx = psi_term(ax, dey_dx, p_zx);
+          P[P_HZX * vol + c] = p_zx;
+        }
+        hz[c] = hz0 + dt_mu * (ty - tx);
+      }
     }
     if (fl & (F_HPTS | F_MON)) {
       __syncthreads();
-      T* hs[3] = {d.f[3], d.f[4], d.f[5]};
+      T* hs[3] = {hx, hy, hz};
       if (fl & F_HPTS)
         for (int t = 3; t < 6; ++t) {
           const int np_ = t == 3 ? d.n_mx : (t == 4 ? d.n_my : d.n_mz);
           for (int q = d.off[t][cta] + tid; q < d.off[t][cta + 1]; q += NT) {
             const Pt3 p = d.pts[t][q];
-            atomicAdd(hs[t - 3] + at(d, p.i, p.j, p.k), -(d.dt_mu * wave(d, t, np_, p.m, n, sub)));
+            atomicAdd(hs[t - 3] + at(d, p.i, p.j, p.k), -(dt_mu * wave(d, t, np_, p.m, n, sub)));
           }
         }
       if (fl & F_MON) {
@@ -262,59 +319,6 @@ __global__ void __launch_bounds__(NT) yee_h(Dev3<T> d, int sub) {
         if (live) write_monitors(d, 3, 6, n, cta, i, j, k);
       }
     }
-  }
-}
-
-// E at one cell of plane i (fdtd3d.py:596-626); for the port edge it also
-// leaves Ez^n, curl_z and the plain update in `s_port`.
-template <typename T, bool CP>
-__device__ __forceinline__ void e_cell(const Dev3<T>& d, int i, int j, int k, long long c,
-                                       bool port_here, T* s_port) {
-  const int nx = d.nx, ny = d.ny, nz = d.nz;
-  T *ex = d.f[0], *ey = d.f[1], *ez = d.f[2];
-  const T *hx = d.f[3], *hy = d.f[4], *hz = d.f[5];
-  const long long dj = d.sz, di = (long long)d.sy * d.sz;
-  const long long g = ((long long)i * ny + j) * nz + k;  // node coefficients
-  const T hx_c = hx[c], hy_c = hy[c], hz_c = hz[c];
-  // Ex (nx-1, ny, nz) interior j, k: t_exy - t_exz
-  if (i < nx - 1 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2) {
-    const T dhz_dy = (hz_c - hz[c - dj]) * d.inv_d[1];
-    const T dhy_dz = (hy_c - hy[c - 1]) * d.inv_d[2];
-    T ty = dhz_dy, tz = dhy_dz;
-    if constexpr (CP) {
-      ty = cpml<T, true>(d, 1, j - 1, ny - 2, dhz_dy, d.psi + P_EXY * d.vol + c);
-      tz = cpml<T, true>(d, 2, k - 1, nz - 2, dhy_dz, d.psi + P_EXZ * d.vol + c);
-    }
-    ex[c] = d.ca[g] * ex[c] + d.cb[g] * (ty - tz);
-  }
-  // Ey (nx, ny-1, nz) interior i, k: t_eyz - t_eyx
-  if (i >= 1 && i <= nx - 2 && j < ny - 1 && k >= 1 && k <= nz - 2) {
-    const T dhx_dz = (hx_c - hx[c - 1]) * d.inv_d[2];
-    const T dhz_dx = (hz_c - hz[c - di]) * d.inv_d[0];
-    T tz = dhx_dz, tx = dhz_dx;
-    if constexpr (CP) {
-      tz = cpml<T, true>(d, 2, k - 1, nz - 2, dhx_dz, d.psi + P_EYZ * d.vol + c);
-      tx = cpml<T, true>(d, 0, i - 1, nx - 2, dhz_dx, d.psi + P_EYX * d.vol + c);
-    }
-    ey[c] = d.ca[g] * ey[c] + d.cb[g] * (tz - tx);
-  }
-  // Ez (nx, ny, nz-1) interior i, j: t_ezx - t_ezy
-  if (i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k < nz - 1) {
-    const T dhy_dx = (hy_c - hy[c - di]) * d.inv_d[0];
-    const T dhx_dy = (hx_c - hx[c - dj]) * d.inv_d[1];
-    T tx = dhy_dx, ty = dhx_dy;
-    if constexpr (CP) {
-      tx = cpml<T, true>(d, 0, i - 1, nx - 2, dhy_dx, d.psi + P_EZX * d.vol + c);
-      ty = cpml<T, true>(d, 1, j - 1, ny - 2, dhx_dy, d.psi + P_EZY * d.vol + c);
-    }
-    const T curl = tx - ty;
-    const T upd = d.ca[g] * ez[c] + d.cb[g] * curl;
-    if (port_here && i == d.pi && j == d.pj && k == d.pk) {
-      s_port[0] = ez[c];
-      s_port[1] = curl;
-      s_port[2] = upd;
-    }
-    ez[c] = upd;
   }
 }
 
@@ -333,20 +337,86 @@ __global__ void __launch_bounds__(NT) yee_e(Dev3<T> d, int sub) {
   const int tid = threadIdx.y * BK + threadIdx.x;
   const int i1 = min(nx, int(blockIdx.z + 1) * NI);
   long long c = at(d, int(blockIdx.z) * NI, j, k);
-  const long long di = (long long)d.sy * d.sz;
+  const long long di = (long long)d.sy * d.sz, dj = d.sz, vol = d.vol;
+  T *ex = d.f[0], *ey = d.f[1], *ez = d.f[2];
+  const T *hx = d.f[3], *hy = d.f[4], *hz = d.f[5];
+  T* P = d.psi;
+  const T idx = d.inv_d[0], idy = d.inv_d[1], idz = d.inv_d[2];
+  // E-type samples of this thread's y and z (the PEC interior, node - 1).
+  Ax<T> ay, az;
+  ay.on = slab_coef<T, true>(d, 1, j - 1, ny - 2, ay.b, ay.c, ay.ik);
+  az.on = slab_coef<T, true>(d, 2, k - 1, nz - 2, az.b, az.c, az.ik);
   for (int i = blockIdx.z * NI; i < i1; ++i, c += di) {
     const int cta = (i * d.gj + blockIdx.y) * d.gk + blockIdx.x;
     const unsigned fl = d.cls[cta];
     const bool port_here = d.has_port && cta == d.port_cta;
     if (live) {
-      if (fl & F_CPML)
-        e_cell<T, true>(d, i, j, k, c, port_here, s_port);
-      else
-        e_cell<T, false>(d, i, j, k, c, port_here, s_port);
+      Ax<T> ax;
+      ax.on = slab_coef<T, true>(d, 0, i - 1, nx - 2, ax.b, ax.c, ax.ik);
+      const long long g = ((long long)i * ny + j) * nz + k;  // node coefficients
+      const T hx0 = hx[c], hy0 = hy[c], hz0 = hz[c];
+      const T hzj = hz[c - dj], hyk = hy[c - 1], hxk = hx[c - 1];
+      const T hzi = hz[c - di], hyi = hy[c - di], hxj = hx[c - dj];
+      const T ex0 = ex[c], ey0 = ey[c], ez0 = ez[c];
+      const T ca = d.ca[g], cb = d.cb[g];
+      const bool vx = i < nx - 1 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2;
+      const bool vy = i >= 1 && i <= nx - 2 && j < ny - 1 && k >= 1 && k <= nz - 2;
+      const bool vz = i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k < nz - 1;
+      T p_xy = T(0), p_xz = T(0), p_yz = T(0), p_yx = T(0), p_zx = T(0), p_zy = T(0);
+      if (vx && ay.on) p_xy = P[P_EXY * vol + c];
+      if (vx && az.on) p_xz = P[P_EXZ * vol + c];
+      if (vy && az.on) p_yz = P[P_EYZ * vol + c];
+      if (vy && ax.on) p_yx = P[P_EYX * vol + c];
+      if (vz && ax.on) p_zx = P[P_EZX * vol + c];
+      if (vz && ay.on) p_zy = P[P_EZY * vol + c];
+      if (vx) {  // Ex (nx-1, ny, nz) interior j, k: t_exy - t_exz
+        const T dhz_dy = (hz0 - hzj) * idy, dhy_dz = (hy0 - hyk) * idz;
+        T ty = dhz_dy, tz = dhy_dz;
+        if (ay.on) {
+          ty = psi_term(ay, dhz_dy, p_xy);
+          P[P_EXY * vol + c] = p_xy;
+        }
+        if (az.on) {
+          tz = psi_term(az, dhy_dz, p_xz);
+          P[P_EXZ * vol + c] = p_xz;
+        }
+        ex[c] = ca * ex0 + cb * (ty - tz);
+      }
+      if (vy) {  // Ey (nx, ny-1, nz) interior i, k: t_eyz - t_eyx
+        const T dhx_dz = (hx0 - hxk) * idz, dhz_dx = (hz0 - hzi) * idx;
+        T tz = dhx_dz, tx = dhz_dx;
+        if (az.on) {
+          tz = psi_term(az, dhx_dz, p_yz);
+          P[P_EYZ * vol + c] = p_yz;
+        }
+        if (ax.on) {
+          tx = psi_term(ax, dhz_dx, p_yx);
+          P[P_EYX * vol + c] = p_yx;
+        }
+        ey[c] = ca * ey0 + cb * (tz - tx);
+      }
+      if (vz) {  // Ez (nx, ny, nz-1) interior i, j: t_ezx - t_ezy
+        const T dhy_dx = (hy0 - hyi) * idx, dhx_dy = (hx0 - hxj) * idy;
+        T tx = dhy_dx, ty = dhx_dy;
+        if (ax.on) {
+          tx = psi_term(ax, dhy_dx, p_zx);
+          P[P_EZX * vol + c] = p_zx;
+        }
+        if (ay.on) {
+          ty = psi_term(ay, dhx_dy, p_zy);
+          P[P_EZY * vol + c] = p_zy;
+        }
+        const T curl = tx - ty;
+        const T upd = ca * ez0 + cb * curl;
+        if (port_here && i == d.pi && j == d.pj && k == d.pk) {
+          s_port[0] = ez0;
+          s_port[1] = curl;
+          s_port[2] = upd;
+        }
+        ez[c] = upd;
+      }
     }
     if (fl & F_EPTS) {
-      T *ex = d.f[0], *ey = d.f[1], *ez = d.f[2];
-      const T *hx = d.f[3], *hy = d.f[4];
       __syncthreads();
       T* es[3] = {ez, ex, ey};  // point types 0 src (Jz), 1 jx, 2 jy
       const T* cbs[3] = {d.cb_src, d.cb_jx, d.cb_jy};
@@ -367,7 +437,6 @@ __global__ void __launch_bounds__(NT) yee_e(Dev3<T> d, int sub) {
                          (src != T(0) ? src * (d.b_port / d.cb[((long long)d.pi * ny + d.pj) * nz + d.pk]) : T(0));
         ez[cp] = ez_new;
         d.out_v[n] = T(-0.5) * d.dz * (s_port[0] + ez_new);
-        const long long dj = d.sz;
         d.out_i[n] = (hy[cp] - hy[cp - di]) * d.dy + (hx[cp - dj] - hx[cp]) * d.dx;
       }
       __syncthreads();
