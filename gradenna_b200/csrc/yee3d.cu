@@ -9,15 +9,18 @@
 //
 // B200 design: two kernels per step updating in place (the H kernel reads
 // only E and the E kernel only H, so no CTA ever reads a value another CTA is
-// writing). A CTA covers a 1 x 8 x 32 (i, j, k) box with k contiguous, so
-// every field access is a coalesced row. CPML psi lives in full padded
-// volumes (zero outside the slabs) indexed like the fields; only slab cells
-// touch them. Point work (sources, the port, probes) is binned by CTA box on
-// the host and applied by the owning CTA after its sweep. The running DFT
-// uses the monitor ring of the 2D path: each step the owning CTA writes the
-// monitored cells to ring slot n % R, and one fold kernel per R steps adds
-// sum_t ph[t,k] x_t to the accumulators. One chunk of R steps is captured as
-// a CUDA graph and replayed; kernels read the absolute step from a counter.
+// writing). A CTA covers an 8 x 32 (j, k) tile with k contiguous, so every
+// field access is a coalesced row, and walks 8 consecutive i-planes. Each
+// thread loads all operands of its cell before updating it. CPML psi lives
+// in full padded volumes (zero outside the slabs) indexed like the fields;
+// only slab cells touch them, on per-thread slab flags. Point work (sources,
+// the port, probes) is binned by plane box on the host and applied by the
+// owning CTA after its sweep; per plane-box flags keep the other boxes on the
+// bare stencil. The running DFT uses the monitor ring of the 2D path: after
+// each half step a gather kernel copies the monitored cells to ring slot
+// n % R, and one fold kernel per R steps adds sum_t ph[t,k] x_t to the
+// accumulators. One chunk of R steps is captured as a CUDA graph and
+// replayed; kernels read the absolute step from a counter.
 #include <algorithm>
 #include <array>
 #include <cmath>
@@ -36,14 +39,6 @@ struct Pt3 {
   int m, i, j, k;
 };
 
-// One monitor's part inside one CTA box (a single i-plane): cells j in
-// [j0, j1), k in [k0, k1) of component comp go to ring index
-// base + (i * s1 + j) * s2 + k. Binned per CTA on the host.
-struct MonW3 {
-  int j0, j1, k0, k1, comp, s2;
-  long long base;
-  int s1, pad;
-};
 constexpr int MAXF = 64;  // monitors whose offsets the fold stages in shared memory
 
 struct Mon3 {
@@ -80,8 +75,13 @@ struct Dev3 {
   long long mon_cells;
   int n_mons;
   const Mon3* mons;
-  const int* mw_off;  // per-CTA CSR over mw
-  const MonW3* mw;
+  // Monitor cells split by field kind for the ring gathers: side 0 = E
+  // components, 1 = H; gmon[side] lists that side's monitors, gcum[side] the
+  // running count of their cells (gn[side] + 1 entries).
+  const int* gmon[2];
+  const long long* gcum[2];
+  int gn[2];
+  long long gcells[2];
   const unsigned char* cls;  // per plane-box work flags (F_*)
   T* cwv;                // CW source values of the chunk: [sub][cw_off[type] + m]
   long long cw_total, cw_off[6];
@@ -132,48 +132,37 @@ __global__ void yee_cw_synth(Dev3<T> d, int cnt) {
   }
 }
 
-// CPML term of one derivative along axis `ax` at sample index `s` of that
-// axis (E-type: s = node - 1 on the PEC interior of n-2 samples; H-type: s
-// on the n-1 half samples): psi <- b psi + c diff, returns diff/kappa + psi
-// inside a slab and diff outside (cpml.py:120-158).
-template <typename T, bool E>
-__device__ __forceinline__ T cpml(const Dev3<T>& d, int ax, int s, int n_samples, T diff,
-                                  T* psi) {
-  const int m = d.npml;
-  if (s < m) {
-    const T p = (E ? d.be_lo[ax][s] : d.bh_lo[ax][s]) * *psi +
-                (E ? d.ce_lo[ax][s] : d.ch_lo[ax][s]) * diff;
-    *psi = p;
-    return diff * (E ? d.ik_e[ax][s] : d.ik_h[ax][s]) + p;
-  }
-  if (s >= n_samples - m) {
-    const int t = s - (n_samples - m);
-    const T p = (E ? d.be_hi[ax][t] : d.bh_hi[ax][t]) * *psi +
-                (E ? d.ce_hi[ax][t] : d.ch_hi[ax][t]) * diff;
-    *psi = p;
-    return diff * (E ? d.ik_e[ax][s] : d.ik_h[ax][s]) + p;
-  }
-  return diff;
-}
-
-// Monitored cells of this CTA's box for components in [c0, c1): only the
-// monitor parts binned to this CTA.
+// Monitor ring writes of step n (fdtd3d.py:635-662, the running DFT's
+// samples): after the H (side 1) or the E (side 0) half step, one thread per
+// monitored cell of that side copies the field value into ring slot n % R.
+// Doing this in its own launch keeps the per-cell stencil kernels free of
+// monitor bookkeeping; the ring traffic is O(monitored cells).
 template <typename T>
-__device__ __forceinline__ void write_monitors(const Dev3<T>& d, int c0, int c1, int n, int cta,
-                                               int i, int j, int k) {
-  const int qb = d.mw_off[cta], qe = d.mw_off[cta + 1];
-  if (qb == qe) return;
-  T* slot = d.mring + (long long)(n % d.R) * d.mon_cells;
-  for (int q = qb; q < qe; ++q) {
-    const MonW3 w = d.mw[q];
-    if (w.comp < c0 || w.comp >= c1 || j < w.j0 || j >= w.j1 || k < w.k0 || k >= w.k1) continue;
-    slot[w.base + ((long long)i * w.s1 + j) * w.s2 + k] = d.f[w.comp][at(d, i, j, k)];
+__global__ void __launch_bounds__(256) yee_gather(Dev3<T> d, int sub, int side) {
+  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= d.gcells[side]) return;
+  const long long* cum = d.gcum[side];
+  int lo = 0, hi = d.gn[side] - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (cum[mid] <= r)
+      lo = mid;
+    else
+      hi = mid - 1;
   }
+  const Mon3 m = d.mons[d.gmon[side][lo]];
+  const long long loc = r - cum[lo];
+  const int k = int(loc % m.s2);
+  const long long t = loc / m.s2;
+  const int j = int(t % m.s1), i = int(t / m.s1);
+  const int n = *d.step_base + sub;
+  d.mring[(long long)(n % d.R) * d.mon_cells + m.off + loc] =
+      d.f[m.comp][at(d, m.lo0 + i, m.lo1 + j, m.lo2 + k)];
 }
 
 // Per plane-box flags (bit set = the box needs that work), computed on the
 // host so that most boxes run the bare stencil with no per-thread checks.
-enum : unsigned char { F_HPTS = 1, F_EPTS = 2, F_MON = 4, F_CPML = 8 };
+enum : unsigned char { F_HPTS = 1, F_EPTS = 2, F_CPML = 8 };
 
 // Planes per CTA: a CTA walks NI consecutive i-planes of its (j, k) tile.
 constexpr int NI = 8;
@@ -303,20 +292,15 @@ __global__ void __launch_bounds__(NT) yee_h(Dev3<T> d, int sub) {
         hz[c] = hz0 + dt_mu * (ty - tx);
       }
     }
-    if (fl & (F_HPTS | F_MON)) {
+    if (fl & F_HPTS) {
       __syncthreads();
       T* hs[3] = {hx, hy, hz};
-      if (fl & F_HPTS)
-        for (int t = 3; t < 6; ++t) {
-          const int np_ = t == 3 ? d.n_mx : (t == 4 ? d.n_my : d.n_mz);
-          for (int q = d.off[t][cta] + tid; q < d.off[t][cta + 1]; q += NT) {
-            const Pt3 p = d.pts[t][q];
-            atomicAdd(hs[t - 3] + at(d, p.i, p.j, p.k), -(dt_mu * wave(d, t, np_, p.m, n, sub)));
-          }
+      for (int t = 3; t < 6; ++t) {
+        const int np_ = t == 3 ? d.n_mx : (t == 4 ? d.n_my : d.n_mz);
+        for (int q = d.off[t][cta] + tid; q < d.off[t][cta + 1]; q += NT) {
+          const Pt3 p = d.pts[t][q];
+          atomicAdd(hs[t - 3] + at(d, p.i, p.j, p.k), -(dt_mu * wave(d, t, np_, p.m, n, sub)));
         }
-      if (fl & F_MON) {
-        __syncthreads();
-        if (live) write_monitors(d, 3, 6, n, cta, i, j, k);
       }
     }
   }
@@ -444,10 +428,6 @@ __global__ void __launch_bounds__(NT) yee_e(Dev3<T> d, int sub) {
         const Pt3 p = d.pts[6][q];
         d.out_probe[(long long)n * d.n_probes + p.m] = ez[at(d, p.i, p.j, p.k)];
       }
-    }
-    if (fl & F_MON) {
-      __syncthreads();
-      if (live) write_monitors(d, 0, 3, n, cta, i, j, k);
     }
   }
 }
@@ -626,8 +606,8 @@ static void comp_shape(int c, int nx, int ny, int nz, int s[3]) {
 
 struct Layout3 {
   int sy = 0, sz = 0, gj = 0, gk = 0, n_cta = 0, R = 32;
-  long long vol = 0, mon_cells = 0, n_mw = 0;
-  size_t fields, psi, zero_end, off[7], pts[7], mons, mw_off, mw, mring, step, eacc, cwv, cls,
+  long long vol = 0, mon_cells = 0;
+  size_t fields, psi, zero_end, off[7], pts[7], mons, gmon, gcum, mring, step, eacc, cwv, cls,
       total;
 };
 
@@ -651,16 +631,6 @@ static std::vector<std::array<int, 7>> mon_boxes3(const GdnYeeParams* p,
                  g.hi[2] - g.lo[2]});
   }
   return v;
-}
-
-// (CTA, monitor) parts: every i-plane x (j, k) CTA tile a monitor box crosses.
-static long long mon_parts3(const GdnYeeParams* p, const GdnYeePoints* pts) {
-  long long n = 0;
-  for (const auto& b : mon_boxes3(p, pts))
-    if (b[4] > 0 && b[5] > 0 && b[6] > 0)
-      n += (long long)b[4] * ((b[2] + b[5] - 1) / BJ - b[2] / BJ + 1) *
-           ((b[3] + b[6] - 1) / BK - b[3] / BK + 1);
-  return n;
 }
 
 static long long mon_cells3(const GdnYeeParams* p, const GdnYeePoints* pts) {
@@ -699,7 +669,6 @@ static Layout3 make_layout3(const GdnYeeParams* p, const GdnYeePoints* pts, size
   L.gj = int(div_up(p->ny, BJ));
   L.n_cta = p->nx * L.gj * L.gk;
   L.mon_cells = pts ? mon_cells3(p, pts) : 0;
-  L.n_mw = pts ? mon_parts3(p, pts) : 0;
   const size_t budget = size_t(2) << 30;
   long long r = L.mon_cells > 0 ? (long long)(budget / (size_t(L.mon_cells) * esize)) : 32;
   L.R = int(std::max<long long>(1, std::min<long long>(32, r)));
@@ -713,8 +682,9 @@ static Layout3 make_layout3(const GdnYeeParams* p, const GdnYeePoints* pts, size
     L.pts[t] = cv.take<Pt3>(std::max(count_of(p, t), 1));
   }
   L.mons = cv.take<Mon3>(std::max(p->n_monitors, 6));
-  L.mw_off = cv.take<int>(L.n_cta + 1);
-  L.mw = cv.take<MonW3>(size_t(std::max<long long>(L.n_mw, 1)));
+  const int nmon = std::max(p->n_monitors, 6);
+  L.gmon = cv.take<int>(2 * size_t(nmon));
+  L.gcum = cv.take<long long>(2 * size_t(nmon + 1));
   L.mring = cv.take<char>(std::max<size_t>(size_t(L.mon_cells) * L.R, 1) * esize);
   L.eacc = cv.take<double>(p->record_energy ? 2 * size_t(std::max(p->n_steps, 1)) : 1);
   long long cw_total = 0;
@@ -942,50 +912,37 @@ static int run3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuff
       ++k;
     }
   }
-  // Monitor parts per CTA (CSR over CTA ids (i * gj + j / BJ) * gk + k / BK).
-  std::vector<int> mon_off;
+  // Gather tables: the E-side and the H-side monitors with running cell counts.
   {
-    std::vector<int> cnt(L.n_cta + 1, 0);
-    auto for_parts = [&](auto&& fn) {
-      for (const Mon3& m : mons) {
-        if (m.count <= 0) continue;
-        for (int i = m.lo0; i < m.lo0 + m.s0; ++i)
-          for (int by = m.lo1 / BJ; by <= (m.lo1 + m.s1 - 1) / BJ; ++by)
-            for (int bx = m.lo2 / BK; bx <= (m.lo2 + m.s2 - 1) / BK; ++bx) {
-              MonW3 w{};
-              w.j0 = std::max(m.lo1, by * BJ);
-              w.j1 = std::min(m.lo1 + m.s1, (by + 1) * BJ);
-              w.k0 = std::max(m.lo2, bx * BK);
-              w.k1 = std::min(m.lo2 + m.s2, (bx + 1) * BK);
-              w.comp = m.comp;
-              w.s1 = m.s1;
-              w.s2 = m.s2;
-              w.base = m.off - ((long long)m.lo0 * m.s1 + m.lo1) * m.s2 - m.lo2;
-              fn((i * L.gj + by) * L.gk + bx, w);
-            }
+    const int nmon = std::max(p->n_monitors, 6);
+    std::vector<int> gm(2 * size_t(nmon), 0);
+    std::vector<long long> gc(2 * size_t(nmon + 1), 0);
+    for (int side = 0; side < 2; ++side) {
+      int q = 0;
+      long long cum = 0;
+      for (int mi = 0; mi < int(mons.size()); ++mi) {
+        if ((mons[mi].comp >= 3) != (side == 1) || mons[mi].count <= 0) continue;
+        gm[side * nmon + q] = mi;
+        gc[side * (nmon + 1) + q] = cum;
+        cum += mons[mi].count;
+        ++q;
       }
-    };
-    for_parts([&](int c, const MonW3&) { cnt[c + 1]++; });
-    for (int c = 0; c < L.n_cta; ++c) cnt[c + 1] += cnt[c];
-    if ((long long)cnt[L.n_cta] != L.n_mw)
-      GDN_BAD_ARG("internal: %d monitor parts, layout sized for %lld", cnt[L.n_cta], L.n_mw);
-    std::vector<MonW3> mw(std::max<long long>(L.n_mw, 1));
-    std::vector<int> cur(cnt.begin(), cnt.end() - 1);
-    for_parts([&](int c, const MonW3& w) { mw[cur[c]++] = w; });
-    GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.mw_off, cnt.data(), cnt.size() * sizeof(int),
+      gc[side * (nmon + 1) + q] = cum;
+      d.gn[side] = q;
+      d.gcells[side] = cum;
+      d.gmon[side] = reinterpret_cast<const int*>(ws + L.gmon) + side * nmon;
+      d.gcum[side] = reinterpret_cast<const long long*>(ws + L.gcum) + side * (nmon + 1);
+    }
+    GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.gmon, gm.data(), gm.size() * sizeof(int),
                                  cudaMemcpyHostToDevice, stream));
-    mon_off = cnt;
-    if (L.n_mw > 0)
-      GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.mw, mw.data(), size_t(L.n_mw) * sizeof(MonW3),
-                                   cudaMemcpyHostToDevice, stream));
-    d.mw_off = reinterpret_cast<const int*>(ws + L.mw_off);
-    d.mw = reinterpret_cast<const MonW3*>(ws + L.mw);
+    GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.gcum, gc.data(), gc.size() * sizeof(long long),
+                                 cudaMemcpyHostToDevice, stream));
   }
   d.n_mons = int(mons.size());
   d.mons = reinterpret_cast<const Mon3*>(ws + L.mons);
   // Work flags per plane box: points of the H or E kernel (the port's box
-  // counts as E points), monitor parts, and any CPML slab within reach of
-  // the box (either field type, a margin of one cell).
+  // counts as E points) and any CPML slab within reach of the box (either
+  // field type, a margin of one cell).
   {
     std::vector<unsigned char> cls(L.n_cta, 0);
     for (int t = 0; t < 7; ++t) {
@@ -996,8 +953,6 @@ static int run3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuff
             (t >= 3 && t <= 5) ? F_HPTS : F_EPTS;
     }
     if (p->has_port) cls[d.port_cta] |= F_EPTS;
-    for (int c = 0; c < L.n_cta; ++c)
-      if (mon_off[c + 1] > mon_off[c]) cls[c] |= F_MON;
     const int m = p->npml;
     auto near_slab = [m](int lo, int hi, int n) {  // cells [lo, hi) of an axis of n nodes
       return lo <= m + 1 || hi - 1 >= n - 2 - m;
@@ -1036,10 +991,20 @@ static int run3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuff
       yee_cw_synth<T><<<unsigned(div_up(d.cw_total, 256)), 256, 0, s>>>(d, cnt);
       ++k;
     }
+    const unsigned gb0 = unsigned(div_up(d.gcells[0], 256)), gb1 = unsigned(div_up(d.gcells[1], 256));
     for (int t = 0; t < cnt; ++t) {
       yee_h<T><<<grd, blk, 0, s>>>(d, t);
+      k += 1;
+      if (gb1 > 0) {
+        yee_gather<T><<<gb1, 256, 0, s>>>(d, t, 1);
+        ++k;
+      }
       yee_e<T><<<grd, blk, 0, s>>>(d, t);
-      k += 2;
+      k += 1;
+      if (gb0 > 0) {
+        yee_gather<T><<<gb0, 256, 0, s>>>(d, t, 0);
+        ++k;
+      }
       if (p->record_energy) {
         yee_energy<T><<<eblocks, 256, 0, s>>>(d, eacc, t);
         ++k;
