@@ -842,11 +842,12 @@ static Cfg pick_cfg(const GdnTmParams* p, size_t esize, int force = -1) {
   if (force >= 0 && force < NCFG) return c[force];
   const char* env = getenv("GDN_TM_TILE");
   if (env && env[0] >= '0' && env[0] < '0' + NCFG && env[1] == 0) return c[env[0] - '0'];
-  // Measured on B200 (f32): 64x64 tiles win once they give every SM a tile
-  // (1024^2: 129 vs 119/125 Gcell-steps/s); below that the 16x32 tiles keep
-  // more SMs busy (512^2: 47 vs 34; 140^2: 5.1 vs 2.7).
+  // Measured on B200 (f32, forward + adjoint at 1024^2 with the general
+  // tiles skipping psi outside the slabs): 32x64 tiles 109 Gcell-steps/s,
+  // 16x32 106, 64x64 102. Below a tile per SM for the 64x64 shape the 16x32
+  // tiles keep more SMs busy (512^2: 47 vs 34; 140^2: 5.1 vs 2.7).
   const long long big = div_up(p->nx, c[0].ti) * div_up(p->ny, c[0].tj);
-  return big >= 148 ? c[0] : c[2];
+  return big >= 148 ? c[1] : c[2];
 }
 
 // Monitor boxes {comp, lo0, lo1, h, w} in ring order: the listed boxes, or

@@ -106,8 +106,18 @@ __device__ __forceinline__ T wave(const Dev3<T>& d, int type, int n_pts, int m, 
 
 // CW source values J(n) = env[n] Re(sum_k W_k conj(ph[n,k])) of every point
 // for the `cnt` steps of a chunk, once per chunk instead of once per step.
+// The chunk's phase rows are staged in shared memory and each point's K
+// weights are held in registers.
 template <typename T>
-__global__ void yee_cw_synth(Dev3<T> d, int cnt) {
+__global__ void __launch_bounds__(256) yee_cw_synth(Dev3<T> d, int cnt) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  double2* sph = reinterpret_cast<double2*>(smem_raw);  // [2][cnt][K]: E-type, H-type
+  const int n0 = *d.step_base, K = d.n_freq;
+  for (int q = threadIdx.x; q < cnt * K; q += blockDim.x) {
+    sph[q] = d.ph_e[(long long)n0 * K + q];
+    sph[cnt * K + q] = d.ph_h[(long long)n0 * K + q];
+  }
+  __syncthreads();
   const long long mg = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (mg >= d.cw_total) return;
   int type = 0;
@@ -119,15 +129,18 @@ __global__ void yee_cw_synth(Dev3<T> d, int cnt) {
 #pragma unroll
   for (int t = 1; t < 6; ++t)
     if (type == t) w = d.w[t];
-  const double2* ph = type <= 2 ? d.ph_e : d.ph_h;
-  const int n0 = *d.step_base, K = d.n_freq;
+  const double2* ph = sph + (type <= 2 ? 0 : cnt * K);
+  double2 wr[KMAX];
+#pragma unroll
+  for (int k = 0; k < KMAX; ++k) wr[k] = k < K ? w[m * K + k] : make_double2(0.0, 0.0);
   for (int t = 0; t < cnt; ++t) {
     double s = 0.0;
-    for (int k = 0; k < K; ++k) {
-      const double2 a = w[m * K + k];
-      const double2 p = ph[(long long)(n0 + t) * K + k];
-      s += a.x * p.x + a.y * p.y;
-    }
+#pragma unroll
+    for (int k = 0; k < KMAX; ++k)
+      if (k < K) {
+        const double2 p = ph[t * K + k];
+        s += wr[k].x * p.x + wr[k].y * p.y;
+      }
     d.cwv[(long long)t * d.cw_total + mg] = T(d.cw_env[n0 + t] * s);
   }
 }
@@ -988,7 +1001,8 @@ static int run3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuff
   auto enqueue = [&](int cnt, cudaStream_t s) -> uint64_t {
     uint64_t k = 0;
     if (d.cw_total > 0) {
-      yee_cw_synth<T><<<unsigned(div_up(d.cw_total, 256)), 256, 0, s>>>(d, cnt);
+      yee_cw_synth<T><<<unsigned(div_up(d.cw_total, 256)), 256,
+                        2 * size_t(cnt) * p->n_freq * sizeof(double2), s>>>(d, cnt);
       ++k;
     }
     const unsigned gb0 = unsigned(div_up(d.gcells[0], 256)), gb1 = unsigned(div_up(d.gcells[1], 256));
