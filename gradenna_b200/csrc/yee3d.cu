@@ -30,11 +30,8 @@
 namespace gdn {
 namespace yee3d {
 
-constexpr int VK = 4;            // cells along k per thread (one 16- or 32-byte vector)
-constexpr int TK = 16, TJ = 16;  // threads along k and j
-constexpr int BK = TK * VK, BJ = TJ;  // CTA box along k and j (one i-plane)
-constexpr int NT = TK * TJ;
-constexpr int KP = 4;  // ghost cells before k = 0 (keeps k-vectors aligned)
+constexpr int BK = 32, BJ = 8;  // CTA box along k and j (one i-plane)
+constexpr int NT = BK * BJ;
 constexpr int KMAX = 16;
 constexpr int NC = 6;  // components: ex ey ez hx hy hz
 
@@ -96,7 +93,7 @@ enum { P_EXY, P_EXZ, P_EYX, P_EYZ, P_EZX, P_EZY, P_HXY, P_HXZ, P_HYX, P_HYZ, P_H
 
 template <typename T>
 __device__ __forceinline__ long long at(const Dev3<T>& d, int i, int j, int k) {
-  return ((long long)(i + 1) * d.sy + (j + 1)) * d.sz + (k + KP);
+  return ((long long)(i + 1) * d.sy + (j + 1)) * d.sz + (k + 1);
 }
 
 // Source value of point m of channel `type` at step n (chunk offset sub):
@@ -190,7 +187,7 @@ __global__ void __launch_bounds__(256) yee_gather(Dev3<T> d, int sub, int side) 
 enum : unsigned char { F_HPTS = 1, F_EPTS = 2, F_CPML = 8 };
 
 // Planes per CTA: a CTA walks NI consecutive i-planes of its (j, k) tile.
-constexpr int NI = 2;
+constexpr int NI = 8;
 
 // CPML coefficients of sample s of axis ax (E-type: the ns = n-2 samples
 // of the PEC interior; H-type: the ns = n-1 half samples). Returns whether
@@ -234,124 +231,88 @@ __device__ __forceinline__ T psi_term(const Ax<T>& a, T diff, T& psi) {
   return diff * a.ik + psi;
 }
 
-// VK consecutive cells along k (an aligned 16-byte float4 or two double2).
-template <typename T>
-__device__ __forceinline__ void ld4(T* o, const T* p) {
-  if constexpr (sizeof(T) == 4) {
-    const float4 a = *reinterpret_cast<const float4*>(p);
-    o[0] = a.x; o[1] = a.y; o[2] = a.z; o[3] = a.w;
-  } else {
-    const double2 a = reinterpret_cast<const double2*>(p)[0];
-    const double2 b = reinterpret_cast<const double2*>(p)[1];
-    o[0] = a.x; o[1] = a.y; o[2] = b.x; o[3] = b.y;
-  }
-}
-template <typename T>
-__device__ __forceinline__ void st4(T* p, const T* v) {
-  if constexpr (sizeof(T) == 4) {
-    *reinterpret_cast<float4*>(p) = make_float4(v[0], v[1], v[2], v[3]);
-  } else {
-    reinterpret_cast<double2*>(p)[0] = make_double2(v[0], v[1]);
-    reinterpret_cast<double2*>(p)[1] = make_double2(v[2], v[3]);
-  }
-}
-
 // ---------------------------------------------------------------------------
 // H update: E^n -> H^{n+1/2} (fdtd3d.py:564-588) + Mx/My/Mz + H monitors.
 // A CTA covers a BJ x BK tile of NI consecutive i-planes.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(NT, 2) yee_h(Dev3<T> d, int sub) {
+__global__ void __launch_bounds__(NT) yee_h(Dev3<T> d, int sub) {
   const int n = *d.step_base + sub;
-  const int k0 = blockIdx.x * BK + threadIdx.x * VK;
+  const int k = blockIdx.x * BK + threadIdx.x;
   const int j = blockIdx.y * BJ + threadIdx.y;
   const int nx = d.nx, ny = d.ny, nz = d.nz;
-  const bool live = j < ny && k0 < nz;
-  const int tid = threadIdx.y * TK + threadIdx.x;
+  const bool live = j < ny && k < nz;
+  const int tid = threadIdx.y * BK + threadIdx.x;
   const int i1 = min(nx, int(blockIdx.z + 1) * NI);
-  long long c = at(d, int(blockIdx.z) * NI, j, k0);
+  long long c = at(d, int(blockIdx.z) * NI, j, k);
   const long long di = (long long)d.sy * d.sz, dj = d.sz, vol = d.vol;
   const T *ex = d.f[0], *ey = d.f[1], *ez = d.f[2];
   T *hx = d.f[3], *hy = d.f[4], *hz = d.f[5];
   T* P = d.psi;
   const T dt_mu = d.dt_mu, idx = d.inv_d[0], idy = d.inv_d[1], idz = d.inv_d[2];
   // This thread's y and z CPML samples (H-type) are fixed over the planes.
-  Ax<T> ay, az[VK];
+  Ax<T> ay, az;
   ay.on = slab_coef<T, false>(d, 1, j, ny - 1, ay.b, ay.c, ay.ik);
-  bool kz[VK], kx[VK];  // k < nz - 1 (Hx, Hy) and k < nz (Hz)
-#pragma unroll
-  for (int e = 0; e < VK; ++e) {
-    az[e].on = slab_coef<T, false>(d, 2, k0 + e, nz - 1, az[e].b, az[e].c, az[e].ik);
-    kz[e] = k0 + e < nz - 1;
-    kx[e] = k0 + e < nz;
-  }
+  az.on = slab_coef<T, false>(d, 2, k, nz - 1, az.b, az.c, az.ik);
   for (int i = blockIdx.z * NI; i < i1; ++i, c += di) {
     const int cta = (i * d.gj + blockIdx.y) * d.gk + blockIdx.x;
     const unsigned fl = d.cls[cta];
     if (live) {
       Ax<T> ax;
       ax.on = slab_coef<T, false>(d, 0, i, nx - 1, ax.b, ax.c, ax.ik);
-      // Every operand first (all inside the padded volumes), then the updates.
-      T ex0[VK], ey0[VK], ez0[VK], ezj[VK], exj[VK], ezi[VK], eyi[VK], hx0[VK], hy0[VK], hz0[VK];
-      ld4(ex0, ex + c); ld4(ey0, ey + c); ld4(ez0, ez + c);
-      ld4(ezj, ez + c + dj); ld4(exj, ex + c + dj);
-      ld4(ezi, ez + c + di); ld4(eyi, ey + c + di);
-      ld4(hx0, hx + c); ld4(hy0, hy + c); ld4(hz0, hz + c);
-      const T eyk4 = ey[c + VK], exk4 = ex[c + VK];
-      const bool jx = j < ny - 1, iy = i < nx - 1;
-#pragma unroll
-      for (int e = 0; e < VK; ++e) {
-        const long long ce = c + e;
-        const T eyk = e + 1 < VK ? ey0[(e + 1) % VK] : eyk4;
-        const T exk = e + 1 < VK ? ex0[(e + 1) % VK] : exk4;
-        if (jx && kz[e]) {  // Hx (nx, ny-1, nz-1): +dt/mu (t_hxz - t_hxy)
-          const T dey_dz = (eyk - ey0[e]) * idz, dez_dy = (ezj[e] - ez0[e]) * idy;
-          T tz = dey_dz, ty = dez_dy;
-          if (az[e].on) {
-            T p_ = P[P_HXZ * vol + ce];
-            tz = psi_term(az[e], dey_dz, p_);
-            P[P_HXZ * vol + ce] = p_;
-          }
-          if (ay.on) {
-            T p_ = P[P_HXY * vol + ce];
-            ty = psi_term(ay, dez_dy, p_);
-            P[P_HXY * vol + ce] = p_;
-          }
-          hx0[e] = hx0[e] + dt_mu * (tz - ty);
+      // Every operand first (all in the padded volumes), then the updates.
+      const T ex0 = ex[c], ey0 = ey[c], ez0 = ez[c];
+      const T eyk = ey[c + 1], ezj = ez[c + dj], ezi = ez[c + di];
+      const T exk = ex[c + 1], exj = ex[c + dj], eyi = ey[c + di];
+      const T hx0 = hx[c], hy0 = hy[c], hz0 = hz[c];
+      const bool vx = j < ny - 1 && k < nz - 1, vy = i < nx - 1 && k < nz - 1,
+                 vz = i < nx - 1 && j < ny - 1;
+      T p_xz = T(0), p_xy = T(0), p_yx = T(0), p_yz = T(0), p_zy = T(0), p_zx = T(0);
+      if (vx && az.on) p_xz = P[P_HXZ * vol + c];
+      if (vx && ay.on) p_xy = P[P_HXY * vol + c];
+      if (vy && ax.on) p_yx = P[P_HYX * vol + c];
+      if (vy && az.on) p_yz = P[P_HYZ * vol + c];
+      if (vz && ay.on) p_zy = P[P_HZY * vol + c];
+      if (vz && ax.on) p_zx = P[P_HZX * vol + c];
+      if (vx) {  // Hx (nx, ny-1, nz-1): +dt/mu (t_hxz - t_hxy)
+        const T dey_dz = (eyk - ey0) * idz, dez_dy = (ezj - ez0) * idy;
+        T tz = dey_dz, ty = dez_dy;
+        if (az.on) {
+          tz = psi_term(az, dey_dz, p_xz);
+          P[P_HXZ * vol + c] = p_xz;
         }
-        if (iy && kz[e]) {  // Hy (nx-1, ny, nz-1): +dt/mu (t_hyx - t_hyz)
-          const T dez_dx = (ezi[e] - ez0[e]) * idx, dex_dz = (exk - ex0[e]) * idz;
-          T tx = dez_dx, tz = dex_dz;
-          if (ax.on) {
-            T p_ = P[P_HYX * vol + ce];
-            tx = psi_term(ax, dez_dx, p_);
-            P[P_HYX * vol + ce] = p_;
-          }
-          if (az[e].on) {
-            T p_ = P[P_HYZ * vol + ce];
-            tz = psi_term(az[e], dex_dz, p_);
-            P[P_HYZ * vol + ce] = p_;
-          }
-          hy0[e] = hy0[e] + dt_mu * (tx - tz);
+        if (ay.on) {
+          ty = psi_term(ay, dez_dy, p_xy);
+          P[P_HXY * vol + c] = p_xy;
         }
-        if (iy && jx && kx[e]) {  // Hz (nx-1, ny-1, nz): +dt/mu (t_hzy - t_hzx)
-          const T dex_dy = (exj[e] - ex0[e]) * idy, dey_dx = (eyi[e] - ey0[e]) * idx;
-          T ty = dex_dy, tx = dey_dx;
-          if (ay.on) {
-            T p_ = P[P_HZY * vol + ce];
-            ty = psi_term(ay, dex_dy, p_);
-            P[P_HZY * vol + ce] = p_;
-          }
-          if (ax.on) {
-            T p_ = P[P_HZX * vol + ce];
-            tx = psi_term(ax, dey_dx, p_);
-            P[P_HZX * vol + ce] = p_;
-          }
-          hz0[e] = hz0[e] + dt_mu * (ty - tx);
-        }
+        hx[c] = hx0 + dt_mu * (tz - ty);
       }
-      // Cells outside a component's grid keep the values just read (zero).
-      st4(hx + c, hx0); st4(hy + c, hy0); st4(hz + c, hz0);
+      if (vy) {  // Hy (nx-1, ny, nz-1): +dt/mu (t_hyx - t_hyz)
+        const T dez_dx = (ezi - ez0) * idx, dex_dz = (exk - ex0) * idz;
+        T tx = dez_dx, tz = dex_dz;
+        if (ax.on) {
+          tx = psi_term(ax, dez_dx, p_yx);
+          P[P_HYX * vol + c] = p_yx;
+        }
+        if (az.on) {
+          tz = psi_term(az, dex_dz, p_yz);
+          P[P_HYZ * vol + c] = p_yz;
+        }
+        hy[c] = hy0 + dt_mu * (tx - tz);
+      }
+      if (vz) {  // Hz (nx-1, ny-1, nz): +dt/mu (t_hzy - t_hzx)
+        const T dex_dy = (exj - ex0) * idy, dey_dx = (eyi - ey0) * idx;
+        T ty = dex_dy, tx = dey_dx;
+        if (ay.on) {
+          ty = psi_term(ay, dex_dy, p_zy);
+          P[P_HZY * vol + c] = p_zy;
+        }
+        if (ax.on) {
+          tx = psi_term(ax, dey_dx, p_zx);
+          P[P_HZX * vol + c] = p_zx;
+        }
+        hz[c] = hz0 + dt_mu * (ty - tx);
+      }
     }
     if (fl & F_HPTS) {
       __syncthreads();
@@ -363,7 +324,6 @@ __global__ void __launch_bounds__(NT, 2) yee_h(Dev3<T> d, int sub) {
           atomicAdd(hs[t - 3] + at(d, p.i, p.j, p.k), -(dt_mu * wave(d, t, np_, p.m, n, sub)));
         }
       }
-      __syncthreads();
     }
   }
 }
@@ -373,33 +333,25 @@ __global__ void __launch_bounds__(NT, 2) yee_h(Dev3<T> d, int sub) {
 // probes, V/I and E monitors. Same CTA geometry as yee_h.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(NT, 2) yee_e(Dev3<T> d, int sub) {
+__global__ void __launch_bounds__(NT) yee_e(Dev3<T> d, int sub) {
   __shared__ T s_port[3];  // Ez^n, curl_z and the plain-updated Ez at the port edge
   const int n = *d.step_base + sub;
-  const int k0 = blockIdx.x * BK + threadIdx.x * VK;
+  const int k = blockIdx.x * BK + threadIdx.x;
   const int j = blockIdx.y * BJ + threadIdx.y;
   const int nx = d.nx, ny = d.ny, nz = d.nz;
-  const bool live = j < ny && k0 < nz;
-  const int tid = threadIdx.y * TK + threadIdx.x;
+  const bool live = j < ny && k < nz;
+  const int tid = threadIdx.y * BK + threadIdx.x;
   const int i1 = min(nx, int(blockIdx.z + 1) * NI);
-  long long c = at(d, int(blockIdx.z) * NI, j, k0);
+  long long c = at(d, int(blockIdx.z) * NI, j, k);
   const long long di = (long long)d.sy * d.sz, dj = d.sz, vol = d.vol;
   T *ex = d.f[0], *ey = d.f[1], *ez = d.f[2];
   const T *hx = d.f[3], *hy = d.f[4], *hz = d.f[5];
   T* P = d.psi;
   const T idx = d.inv_d[0], idy = d.inv_d[1], idz = d.inv_d[2];
   // E-type samples of this thread's y and z (the PEC interior, node - 1).
-  Ax<T> ay, az[VK];
+  Ax<T> ay, az;
   ay.on = slab_coef<T, true>(d, 1, j - 1, ny - 2, ay.b, ay.c, ay.ik);
-  bool kin[VK], kz[VK];  // 1 <= k <= nz - 2 (Ex, Ey) and k < nz - 1 (Ez)
-#pragma unroll
-  for (int e = 0; e < VK; ++e) {
-    const int k = k0 + e;
-    az[e].on = slab_coef<T, true>(d, 2, k - 1, nz - 2, az[e].b, az[e].c, az[e].ik);
-    kin[e] = k >= 1 && k <= nz - 2;
-    kz[e] = k < nz - 1;
-  }
-  const bool jin = j >= 1 && j <= ny - 2;
+  az.on = slab_coef<T, true>(d, 2, k - 1, nz - 2, az.b, az.c, az.ik);
   for (int i = blockIdx.z * NI; i < i1; ++i, c += di) {
     const int cta = (i * d.gj + blockIdx.y) * d.gk + blockIdx.x;
     const unsigned fl = d.cls[cta];
@@ -407,80 +359,68 @@ __global__ void __launch_bounds__(NT, 2) yee_e(Dev3<T> d, int sub) {
     if (live) {
       Ax<T> ax;
       ax.on = slab_coef<T, true>(d, 0, i - 1, nx - 2, ax.b, ax.c, ax.ik);
-      T hx0[VK], hy0[VK], hz0[VK], hzj[VK], hxj[VK], hzi[VK], hyi[VK], ex0[VK], ey0[VK], ez0[VK];
-      ld4(hx0, hx + c); ld4(hy0, hy + c); ld4(hz0, hz + c);
-      ld4(hzj, hz + c - dj); ld4(hxj, hx + c - dj);
-      ld4(hzi, hz + c - di); ld4(hyi, hy + c - di);
-      ld4(ex0, ex + c); ld4(ey0, ey + c); ld4(ez0, ez + c);
-      const T hyk0 = hy[c - 1], hxk0 = hx[c - 1];
-      const long long g0 = ((long long)i * ny + j) * nz + k0;  // node coefficients
-      T ca[VK], cb[VK];
-#pragma unroll
-      for (int e = 0; e < VK; ++e) {
-        const bool in = k0 + e < nz;
-        ca[e] = in ? d.ca[g0 + e] : T(0);
-        cb[e] = in ? d.cb[g0 + e] : T(0);
+      const long long g = ((long long)i * ny + j) * nz + k;  // node coefficients
+      const T hx0 = hx[c], hy0 = hy[c], hz0 = hz[c];
+      const T hzj = hz[c - dj], hyk = hy[c - 1], hxk = hx[c - 1];
+      const T hzi = hz[c - di], hyi = hy[c - di], hxj = hx[c - dj];
+      const T ex0 = ex[c], ey0 = ey[c], ez0 = ez[c];
+      const T ca = d.ca[g], cb = d.cb[g];
+      const bool vx = i < nx - 1 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2;
+      const bool vy = i >= 1 && i <= nx - 2 && j < ny - 1 && k >= 1 && k <= nz - 2;
+      const bool vz = i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k < nz - 1;
+      T p_xy = T(0), p_xz = T(0), p_yz = T(0), p_yx = T(0), p_zx = T(0), p_zy = T(0);
+      if (vx && ay.on) p_xy = P[P_EXY * vol + c];
+      if (vx && az.on) p_xz = P[P_EXZ * vol + c];
+      if (vy && az.on) p_yz = P[P_EYZ * vol + c];
+      if (vy && ax.on) p_yx = P[P_EYX * vol + c];
+      if (vz && ax.on) p_zx = P[P_EZX * vol + c];
+      if (vz && ay.on) p_zy = P[P_EZY * vol + c];
+      if (vx) {  // Ex (nx-1, ny, nz) interior j, k: t_exy - t_exz
+        const T dhz_dy = (hz0 - hzj) * idy, dhy_dz = (hy0 - hyk) * idz;
+        T ty = dhz_dy, tz = dhy_dz;
+        if (ay.on) {
+          ty = psi_term(ay, dhz_dy, p_xy);
+          P[P_EXY * vol + c] = p_xy;
+        }
+        if (az.on) {
+          tz = psi_term(az, dhy_dz, p_xz);
+          P[P_EXZ * vol + c] = p_xz;
+        }
+        ex[c] = ca * ex0 + cb * (ty - tz);
       }
-      const bool ix = i < nx - 1, iin = i >= 1 && i <= nx - 2, jy = j < ny - 1;
-#pragma unroll
-      for (int e = 0; e < VK; ++e) {
-        const long long ce = c + e;
-        const T hyk = e > 0 ? hy0[e > 0 ? e - 1 : 0] : hyk0;
-        const T hxk = e > 0 ? hx0[e > 0 ? e - 1 : 0] : hxk0;
-        if (ix && jin && kin[e]) {  // Ex (nx-1, ny, nz) interior j, k: t_exy - t_exz
-          const T dhz_dy = (hz0[e] - hzj[e]) * idy, dhy_dz = (hy0[e] - hyk) * idz;
-          T ty = dhz_dy, tz = dhy_dz;
-          if (ay.on) {
-            T p_ = P[P_EXY * vol + ce];
-            ty = psi_term(ay, dhz_dy, p_);
-            P[P_EXY * vol + ce] = p_;
-          }
-          if (az[e].on) {
-            T p_ = P[P_EXZ * vol + ce];
-            tz = psi_term(az[e], dhy_dz, p_);
-            P[P_EXZ * vol + ce] = p_;
-          }
-          ex0[e] = ca[e] * ex0[e] + cb[e] * (ty - tz);
+      if (vy) {  // Ey (nx, ny-1, nz) interior i, k: t_eyz - t_eyx
+        const T dhx_dz = (hx0 - hxk) * idz, dhz_dx = (hz0 - hzi) * idx;
+        T tz = dhx_dz, tx = dhz_dx;
+        if (az.on) {
+          tz = psi_term(az, dhx_dz, p_yz);
+          P[P_EYZ * vol + c] = p_yz;
         }
-        if (iin && jy && kin[e]) {  // Ey (nx, ny-1, nz) interior i, k: t_eyz - t_eyx
-          const T dhx_dz = (hx0[e] - hxk) * idz, dhz_dx = (hz0[e] - hzi[e]) * idx;
-          T tz = dhx_dz, tx = dhz_dx;
-          if (az[e].on) {
-            T p_ = P[P_EYZ * vol + ce];
-            tz = psi_term(az[e], dhx_dz, p_);
-            P[P_EYZ * vol + ce] = p_;
-          }
-          if (ax.on) {
-            T p_ = P[P_EYX * vol + ce];
-            tx = psi_term(ax, dhz_dx, p_);
-            P[P_EYX * vol + ce] = p_;
-          }
-          ey0[e] = ca[e] * ey0[e] + cb[e] * (tz - tx);
+        if (ax.on) {
+          tx = psi_term(ax, dhz_dx, p_yx);
+          P[P_EYX * vol + c] = p_yx;
         }
-        if (iin && jin && kz[e]) {  // Ez (nx, ny, nz-1) interior i, j: t_ezx - t_ezy
-          const T dhy_dx = (hy0[e] - hyi[e]) * idx, dhx_dy = (hx0[e] - hxj[e]) * idy;
-          T tx = dhy_dx, ty = dhx_dy;
-          if (ax.on) {
-            T p_ = P[P_EZX * vol + ce];
-            tx = psi_term(ax, dhy_dx, p_);
-            P[P_EZX * vol + ce] = p_;
-          }
-          if (ay.on) {
-            T p_ = P[P_EZY * vol + ce];
-            ty = psi_term(ay, dhx_dy, p_);
-            P[P_EZY * vol + ce] = p_;
-          }
-          const T curl = tx - ty;
-          const T upd = ca[e] * ez0[e] + cb[e] * curl;
-          if (port_here && i == d.pi && j == d.pj && k0 + e == d.pk) {
-            s_port[0] = ez0[e];
-            s_port[1] = curl;
-            s_port[2] = upd;
-          }
-          ez0[e] = upd;
-        }
+        ey[c] = ca * ey0 + cb * (tz - tx);
       }
-      st4(ex + c, ex0); st4(ey + c, ey0); st4(ez + c, ez0);
+      if (vz) {  // Ez (nx, ny, nz-1) interior i, j: t_ezx - t_ezy
+        const T dhy_dx = (hy0 - hyi) * idx, dhx_dy = (hx0 - hxj) * idy;
+        T tx = dhy_dx, ty = dhx_dy;
+        if (ax.on) {
+          tx = psi_term(ax, dhy_dx, p_zx);
+          P[P_EZX * vol + c] = p_zx;
+        }
+        if (ay.on) {
+          ty = psi_term(ay, dhx_dy, p_zy);
+          P[P_EZY * vol + c] = p_zy;
+        }
+        const T curl = tx - ty;
+        const T upd = ca * ez0 + cb * curl;
+        if (port_here && i == d.pi && j == d.pj && k == d.pk) {
+          s_port[0] = ez0;
+          s_port[1] = curl;
+          s_port[2] = upd;
+        }
+        ez[c] = upd;
+      }
     }
     if (fl & F_EPTS) {
       __syncthreads();
@@ -510,7 +450,6 @@ __global__ void __launch_bounds__(NT, 2) yee_e(Dev3<T> d, int sub) {
         const Pt3 p = d.pts[6][q];
         d.out_probe[(long long)n * d.n_probes + p.m] = ez[at(d, p.i, p.j, p.k)];
       }
-      __syncthreads();
     }
   }
 }
@@ -745,7 +684,7 @@ static int count_of(const GdnYeeParams* p, int t) {
 
 static Layout3 make_layout3(const GdnYeeParams* p, const GdnYeePoints* pts, size_t esize) {
   Layout3 L;
-  L.sz = int(div_up(p->nz, VK) * VK + KP + VK);
+  L.sz = int(div_up(p->nz + 2, 4) * 4);
   L.sy = p->ny + 2;
   L.vol = (long long)(p->nx + 2) * L.sy * L.sz;
   L.gk = int(div_up(p->nz, BK));
@@ -1065,7 +1004,7 @@ static int run3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuff
   if (p->record_energy)
     GDN_TRY_CUDA(cudaMemsetAsync(eacc, 0, 2 * size_t(std::max(N, 1)) * sizeof(double), stream));
 
-  const dim3 blk(TK, TJ);
+  const dim3 blk(BK, BJ);
   const dim3 grd(L.gk, L.gj, unsigned(div_up(nx, NI)));
   const int eblocks = int(std::min<long long>(div_up((long long)nx * ny * nz, 256), 148 * 8));
   auto enqueue = [&](int cnt, cudaStream_t s) -> uint64_t {
