@@ -46,6 +46,11 @@ constexpr int THREADS = 128;
 constexpr long long WAIT_LIMIT = 1LL << 22;  // mbarrier polls before giving up
 
 __device__ int g_tc_error = 0;
+// Test hook: when >= 0, the CTAs of the next launches give up at this
+// reduction step as if a stage wait had run out (they wait, bounded, on a
+// barrier nothing arrives at), so the abort path can be exercised on purpose.
+__device__ int g_tc_inject_step = -1;
+constexpr long long INJECT_LIMIT = 1LL << 10;
 
 struct Args {
   const bf16* in;
@@ -118,7 +123,7 @@ __global__ void __launch_bounds__(THREADS) conv_fwd_tc(Args a) {
   // 1024-byte aligned stage base (the swizzle pattern is tied to address bits)
   const unsigned raw = smem_u32(dyn);
   const unsigned base = (raw + 1023u) & ~1023u;
-  __shared__ __align__(8) unsigned long long bars[STAGES];
+  __shared__ __align__(8) unsigned long long bars[STAGES + 1];  // + the never-arriving one
   __shared__ uint32_t tmem_slot;
   __shared__ int abort_flag;
 
@@ -130,7 +135,7 @@ __global__ void __launch_bounds__(THREADS) conv_fwd_tc(Args a) {
   const int nk = (K + TK - 1) / TK;
 
   if (tid == 0) {
-    for (int s = 0; s < STAGES; ++s) mbar_init(smem_u32(&bars[s]), 1);
+    for (int s = 0; s <= STAGES; ++s) mbar_init(smem_u32(&bars[s]), 1);
     abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::);
   }
@@ -187,7 +192,9 @@ __global__ void __launch_bounds__(THREADS) conv_fwd_tc(Args a) {
     }
   };
 
+  const int inject = g_tc_inject_step;
   bool failed = false;
+  int issued = 0;  // steps whose MMAs have been issued and committed
   // Prologue: stages 0 .. STAGES-2.
   for (int t = 0; t < STAGES - 1; ++t) {
     if (t < nk) load(t);
@@ -202,6 +209,12 @@ __global__ void __launch_bounds__(THREADS) conv_fwd_tc(Args a) {
         if (!mbar_wait(smem_u32(&bars[u % STAGES]), (u / STAGES) & 1)) failed = true;
       }
       if (!failed) load(t);
+    }
+    if (c == inject && tid == 0) {
+      // Nothing arrives at bars[STAGES]: this wait runs out.
+      bool ok = false;
+      for (long long i = 0; i < INJECT_LIMIT && !ok; ++i) ok = mbar_try(smem_u32(&bars[STAGES]), 0);
+      if (!ok) failed = true;
     }
     asm volatile("cp.async.commit_group;\n" ::);
     asm volatile("cp.async.wait_group %0;\n" ::"n"(STAGES - 1));
@@ -229,10 +242,14 @@ __global__ void __launch_bounds__(THREADS) conv_fwd_tc(Args a) {
       asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(
           smem_u32(&bars[c % STAGES])));
     }
+    issued = c + 1;
   }
-  // All MMAs done: the last step's commit tracks every earlier MMA.
-  if (!abort_flag && nk > 0) {
-    const int u = nk - 1;
+  // Wait for every MMA issued so far, on the normal path and after an abort
+  // alike: the last commit tracks all earlier MMAs of the issuing thread, and
+  // none may still read shared memory or write TMEM when TMEM is released
+  // and the CTA exits. The wait is bounded like the others.
+  if (issued > 0) {
+    const int u = issued - 1;
     if (!mbar_wait(smem_u32(&bars[u % STAGES]), (u / STAGES) & 1)) atomicExch(&abort_flag, 1);
   }
   asm volatile("cp.async.wait_all;\n" ::);
@@ -407,6 +424,11 @@ extern "C" int gdn_sur_weights_kmajor(const void* w, int32_t Cin, int32_t Cout, 
       static_cast<const bf16*>(w), Cin, Cout, taps, flip, static_cast<bf16*>(wk));
   gdn::count_launches(1);
   GDN_TRY_CUDA(cudaGetLastError());
+  return GDN_OK;
+}
+
+extern "C" int gdn_sur_inject_timeout(int32_t step) {
+  GDN_TRY_CUDA(cudaMemcpyToSymbol(g_tc_inject_step, &step, sizeof(int)));
   return GDN_OK;
 }
 

@@ -61,6 +61,7 @@ _native.register("gdn_sur_conv_fwd_tc", ctypes.c_int,
                  [_v, _i, _i, _i, _i, _i, _i, _i, _v, _v, _i, _i, _f, _v, _i, _i, _v, _v, _i, _i, _v])
 _native.register("gdn_sur_weights_kmajor", ctypes.c_int, [_v, _i, _i, _i, _i, _v, _v])
 _native.register("gdn_sur_status", ctypes.c_int, [ctypes.POINTER(ctypes.c_int32), _i])
+_native.register("gdn_sur_inject_timeout", ctypes.c_int, [_i])
 
 
 def tc_timeouts(reset: bool = True) -> int:

@@ -477,6 +477,13 @@ int gdn_design_backward(const double* theta, const double* filt, const double* n
  * last reset (0 in normal operation); synchronises with the device. */
 int gdn_sur_status(int32_t* timeouts, int32_t reset);
 
+/* Test hook for the abort path of gdn_sur_conv_fwd_tc. With step >= 0 every
+ * CTA of the following tensor-core convolutions gives up at that reduction
+ * step as if a stage wait had run out: it waits (bounded) for the MMAs it
+ * already issued, releases its TMEM, writes no results and is counted by
+ * gdn_sur_status. step = -1 (the default) switches the hook off. */
+int gdn_sur_inject_timeout(int32_t step);
+
 #ifdef __cplusplus
 }
 #endif

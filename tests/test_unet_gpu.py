@@ -185,3 +185,46 @@ def test_tensor_core_flipped_weights_give_input_gradient():
                          0.1, None, 0, 0, out.data_ptr(), None, 0, 0, s))
     torch.cuda.synchronize()
     assert float((o[0] - o[1]).abs().max()) <= 2e-3 * float(o[0].abs().max())
+
+
+@pytest.mark.parametrize("step", [0, 3, 8])
+def test_tensor_core_conv_abort_path(step):
+    """A tensor-core convolution whose bounded wait runs out (injected at
+    reduction step 0, 3 or 8 of 9, with MMAs of earlier steps possibly still
+    in flight) drains them, releases TMEM and returns: the launch writes no
+    results, gdn_sur_status counts it, the context stays usable and the next
+    convolution is correct."""
+    import ctypes
+
+    from gradenna_b200 import _native
+    from gradenna_b200.unet import tc_timeouts
+
+    lib = _native.load()
+    cin, cout, taps, n, h, w = 64, 64, 9, 2, 26, 26  # 9 reduction steps of 64
+    g = torch.Generator(device="cpu").manual_seed(11)
+    x = torch.randn((n, h, w, cin), generator=g).to(torch.bfloat16).cuda()
+    wt = (torch.randn((taps * cin, cout), generator=g) / 24).to(torch.bfloat16).cuda()
+    wk = torch.empty_like(wt)
+    s = ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    _native.check(lib.gdn_sur_weights_kmajor(wt.data_ptr(), cin, cout, taps, 0, wk.data_ptr(), s))
+
+    def conv(fn, wp):
+        out = torch.full((n * h * w, cout), 7.0, dtype=torch.float32, device="cuda")
+        _native.check(fn(x.data_ptr(), cin, 0, n, h, w, cin, taps, wp.data_ptr(), None, cout, 0,
+                         0.1, None, 0, 0, out.data_ptr(), None, 0, 0, s))
+        return out
+
+    tc_timeouts(reset=True)
+    try:
+        _native.check(lib.gdn_sur_inject_timeout(step))
+        bad = conv(lib.gdn_sur_conv_fwd_tc, wk)
+        torch.cuda.synchronize()
+    finally:
+        _native.check(lib.gdn_sur_inject_timeout(-1))
+    assert tc_timeouts(reset=True) == 1
+    assert bool((bad == 7.0).all())  # nothing written
+    good = conv(lib.gdn_sur_conv_fwd_tc, wk)
+    ref = conv(lib.gdn_sur_conv_fwd, wt)
+    torch.cuda.synchronize()
+    assert tc_timeouts(reset=True) == 0
+    assert float((good - ref).abs().max()) <= 2e-3 * float(ref.abs().max())
