@@ -71,6 +71,7 @@ struct Dev3 {
   const double2* w[6];
   const double2 *ph_e, *ph_h;
   T *out_probe, *out_v, *out_i;
+  const int* pcomp;  // E component of each probe (0 ex, 1 ey, 2 ez), or null = Ez
   T* mring;
   long long mon_cells;
   int n_mons;
@@ -448,7 +449,8 @@ __global__ void __launch_bounds__(NT) yee_e(Dev3<T> d, int sub) {
       __syncthreads();
       for (int q = d.off[6][cta] + tid; q < d.off[6][cta + 1]; q += NT) {
         const Pt3 p = d.pts[6][q];
-        d.out_probe[(long long)n * d.n_probes + p.m] = ez[at(d, p.i, p.j, p.k)];
+        const T* pf = d.pcomp ? d.f[d.pcomp[p.m]] : ez;
+        d.out_probe[(long long)n * d.n_probes + p.m] = pf[at(d, p.i, p.j, p.k)];
       }
     }
   }
@@ -629,8 +631,8 @@ static void comp_shape(int c, int nx, int ny, int nz, int s[3]) {
 struct Layout3 {
   int sy = 0, sz = 0, gj = 0, gk = 0, n_cta = 0, R = 32;
   long long vol = 0, mon_cells = 0;
-  size_t fields, psi, zero_end, off[7], pts[7], mons, gmon, gcum, mring, step, eacc, cwv, cls,
-      total;
+  size_t fields, psi, zero_end, off[7], pts[7], pcomp, mons, gmon, gcum, mring, step, eacc, cwv,
+      cls, total;
 };
 
 // Monitor boxes {comp, lo0, lo1, lo2, s0, s1, s2} in ring order: the listed
@@ -703,6 +705,7 @@ static Layout3 make_layout3(const GdnYeeParams* p, const GdnYeePoints* pts, size
     L.off[t] = cv.take<int>(L.n_cta + 1);
     L.pts[t] = cv.take<Pt3>(std::max(count_of(p, t), 1));
   }
+  L.pcomp = cv.take<int>(std::max(p->n_probes, 1));
   L.mons = cv.take<Mon3>(std::max(p->n_monitors, 6));
   const int nmon = std::max(p->n_monitors, 6);
   L.gmon = cv.take<int>(2 * size_t(nmon));
@@ -739,6 +742,11 @@ static int validate3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYe
     comp_shape(comp_of[t], nx, ny, nz, s);
     const int margin = t == 0 ? 1 : 0;
     for (int m = 0; m < n; ++m) {
+      if (t == 6 && pts->probe_comp) {
+        const int c = pts->probe_comp[m];
+        if (c < 0 || c > 2) GDN_BAD_ARG("probe %d: component %d is not an E component", m, c);
+        comp_shape(c, nx, ny, nz, s);
+      }
       const int i = a[3 * m], j = a[3 * m + 1], k = a[3 * m + 2];
       if (i < margin || j < margin || k < 0 || i > s[0] - 1 - margin || j > s[1] - 1 - margin ||
           k > s[2] - 1)
@@ -879,6 +887,12 @@ static int run3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuff
   d.ph_e = reinterpret_cast<const double2*>(b->ph_e);
   d.ph_h = reinterpret_cast<const double2*>(b->ph_h);
   d.out_probe = static_cast<T*>(b->out_probe);
+  d.pcomp = nullptr;
+  if (p->n_probes > 0 && pts->probe_comp) {
+    GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.pcomp, pts->probe_comp, size_t(p->n_probes) * sizeof(int),
+                                 cudaMemcpyHostToDevice, stream));
+    d.pcomp = reinterpret_cast<const int*>(ws + L.pcomp);
+  }
   d.out_v = static_cast<T*>(b->out_v);
   d.out_i = static_cast<T*>(b->out_i);
   d.mring = reinterpret_cast<T*>(ws + L.mring);
@@ -999,7 +1013,16 @@ static int run3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuff
   if (!mons.empty())
     GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.mons, mons.data(), mons.size() * sizeof(Mon3),
                                  cudaMemcpyHostToDevice, stream));
-  GDN_TRY_CUDA(cudaMemsetAsync(ws + L.fields, 0, L.zero_end - L.fields, stream));
+  // Start from rest, or from the caller's state blob (fields, then psi).
+  const size_t fbytes = size_t(NC) * L.vol * sizeof(T), pbytes = size_t(12) * L.vol * sizeof(T);
+  if (b->state_in) {
+    const char* si = static_cast<const char*>(b->state_in);
+    GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.fields, si, fbytes, cudaMemcpyDeviceToDevice, stream));
+    GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.psi, si + fbytes, pbytes, cudaMemcpyDeviceToDevice, stream));
+    GDN_TRY_CUDA(cudaMemsetAsync(ws + L.step, 0, sizeof(int), stream));
+  } else {
+    GDN_TRY_CUDA(cudaMemsetAsync(ws + L.fields, 0, L.zero_end - L.fields, stream));
+  }
   double* eacc = reinterpret_cast<double*>(ws + L.eacc);
   if (p->record_energy)
     GDN_TRY_CUDA(cudaMemsetAsync(eacc, 0, 2 * size_t(std::max(N, 1)) * sizeof(double), stream));
@@ -1094,6 +1117,11 @@ static int run3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuff
     else
       yee_dft_scale<float2><<<blocks, 256, 0, stream>>>(static_cast<float2*>(m.out), cnt, p->dt);
   }
+  if (b->state_out) {
+    char* so = static_cast<char*>(b->state_out);
+    GDN_TRY_CUDA(cudaMemcpyAsync(so, ws + L.fields, fbytes, cudaMemcpyDeviceToDevice, stream));
+    GDN_TRY_CUDA(cudaMemcpyAsync(so + fbytes, ws + L.psi, pbytes, cudaMemcpyDeviceToDevice, stream));
+  }
   if (p->record_energy && N > 0)
     yee_energy_finish<T><<<unsigned(div_up(N, 256)), 256, 0, stream>>>(
         eacc, static_cast<T*>(b->out_energy), N, p->dx * p->dy * p->dz, p->mu0);
@@ -1120,6 +1148,21 @@ extern "C" int gdn_yee_workspace_size(const GdnYeeParams* p, const GdnYeePoints*
     return GDN_ERR_BAD_ARG;
   }
   *bytes = gdn::yee3d::make_layout3(p, pts, f64 ? sizeof(double) : sizeof(float)).total;
+  return GDN_OK;
+}
+
+extern "C" int gdn_yee_state_size(const GdnYeeParams* p, int f64, size_t* bytes) {
+  if (!p || !bytes) {
+    gdn::set_error("null argument");
+    return GDN_ERR_BAD_ARG;
+  }
+  if (std::min({p->nx, p->ny, p->nz}) < 3) {
+    gdn::set_error("invalid grid");
+    return GDN_ERR_BAD_ARG;
+  }
+  const long long sz = gdn::div_up(p->nz + 2, 4) * 4;
+  const long long vol = (long long)(p->nx + 2) * (p->ny + 2) * sz;
+  *bytes = size_t(gdn::yee3d::NC + 12) * size_t(vol) * (f64 ? sizeof(double) : sizeof(float));
   return GDN_OK;
 }
 

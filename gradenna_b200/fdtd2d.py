@@ -142,14 +142,15 @@ def _waveforms(cur, n_steps, n_pts, dtype, device, name):
     return c.contiguous()
 
 
-def phase_tables(freqs, n_steps: int, dt: float):
+def phase_tables(freqs, n_steps: int, dt: float, step0: int = 0):
     """Exact-phase tables exp(-2 pi i f t_n) in float64 (fdtd2d.py:393-398).
 
     Returns (ph_e, ph_h), each complex128 numpy (n_steps, n_freq), with
-    t_n = (n+1) dt and (n+1/2) dt.
+    t_n = (n+1) dt and (n+1/2) dt for the absolute steps n = step0 ..
+    step0 + n_steps - 1 (step0 > 0: the rows of a resumed run).
     """
     f = np.asarray(freqs, np.float64)
-    nn = np.arange(n_steps, dtype=np.float64)
+    nn = np.arange(step0, step0 + n_steps, dtype=np.float64)
     ph_e = np.exp(-2j * np.pi * np.outer(nn + 1.0, f) * dt)
     ph_h = np.exp(-2j * np.pi * np.outer(nn + 0.5, f) * dt)
     return ph_e, ph_h

@@ -60,6 +60,7 @@ class SimResult3D(NamedTuple):
     hy: torch.Tensor
     hz: torch.Tensor
     monitors: list | None = None
+    state: torch.Tensor | None = None
 
 
 def field_energy_3d(ex, ey, ez, hx, hy, hz, eps, grid: Grid3D):
@@ -107,7 +108,8 @@ class YeeParams(ctypes.Structure):
 
 class YeePoints(ctypes.Structure):
     _fields_ = [(n, _native.P_i32) for n in ("src", "jx", "jy", "mx", "my", "mz", "probe")] + [
-        ("port", ctypes.c_int32 * 3), ("monitors", ctypes.POINTER(_native.DftMonitor))]
+        ("port", ctypes.c_int32 * 3), ("monitors", ctypes.POINTER(_native.DftMonitor)),
+        ("probe_comp", _native.P_i32)]
 
 
 V = ctypes.c_void_p
@@ -124,12 +126,15 @@ class YeeBuffers(ctypes.Structure):
                                     "jx_w", "jy_w", "mx_w", "my_w", "mz_w", "ph_e", "ph_h",
                                     "ex", "ey", "ez", "hx", "hy", "hz", "out_probe", "out_v",
                                     "out_i", "out_energy")]
-                + [("dft", V * 6), ("workspace", V), ("workspace_bytes", ctypes.c_size_t)])
+                + [("dft", V * 6), ("workspace", V), ("workspace_bytes", ctypes.c_size_t),
+                   ("state_in", V), ("state_out", V)])
 
 
 _native.register("gdn_yee_workspace_size", ctypes.c_int, [
     ctypes.POINTER(YeeParams), ctypes.POINTER(YeePoints), ctypes.c_int,
     ctypes.POINTER(ctypes.c_size_t)])
+_native.register("gdn_yee_state_size", ctypes.c_int, [
+    ctypes.POINTER(YeeParams), ctypes.c_int, ctypes.POINTER(ctypes.c_size_t)])
 for _name in ("gdn_yee_run_f32", "gdn_yee_run_f64"):
     _native.register(_name, ctypes.c_int, [ctypes.POINTER(YeeParams), ctypes.POINTER(YeePoints),
                                            ctypes.POINTER(YeeBuffers), ctypes.c_void_p])
@@ -175,6 +180,10 @@ def simulate_3d(
     dtype=None,
     device=None,
     cw_sources=None,
+    probe_comp=None,
+    state_in=None,
+    return_state: bool = False,
+    dft_step0: int = 0,
 ) -> SimResult3D:
     """Run a 3D FDTD simulation on the GPU (drop-in for fdtd3d.simulate_3d).
 
@@ -186,6 +195,14 @@ def simulate_3d(
     frequency-domain adjoint's drive), and ``dft_monitors`` = [(comp, lo,
     hi), ...] boxes (several per component allowed) whose spectra come back
     as ``SimResult3D.monitors`` in the same order (``dft`` is then None).
+
+    Resumable runs (additions): ``probe_comp`` (one of 0, 1, 2 per probe)
+    records Ex / Ey / Ez instead of Ez only; ``state_in`` (a uint8 device
+    tensor returned as ``SimResult3D.state`` by an earlier run with
+    ``return_state=True``) starts the run from that state instead of rest;
+    ``dft_step0`` is the absolute index of the run's first step, so that the
+    DFT phases of a resumed run continue the whole run's (its phasors are
+    the partial sums over its own steps). Waveforms are this run's rows.
     """
     nx, ny, nz = grid.nx, grid.ny, grid.nz
     if min(nx, ny, nz) <= 2 * cpml.thickness + 2:
@@ -323,7 +340,7 @@ def simulate_3d(
             np.dtype(np.complex128): torch.complex128}[np.dtype(dft_dtype)]
     ph_e = ph_h = None
     if n_freq:
-        pe, phh = phase_tables(freqs, n_steps, dt)
+        pe, phh = phase_tables(freqs, n_steps, dt, int(dft_step0))
         ph_e = torch.as_tensor(pe, device=dev)
         ph_h = torch.as_tensor(phh, device=dev)
         bufs.ph_e, bufs.ph_h = ph_e.data_ptr(), ph_h.data_ptr()
@@ -345,7 +362,18 @@ def simulate_3d(
 
     # Outputs.
     fields = [torch.empty(s, dtype=fdt, device=dev) for s in shapes]
-    probe_idx = _idx3(probe_ijk, "probe_ijk", shapes[2], 0)
+    if probe_comp is None:
+        probe_idx = _idx3(probe_ijk, "probe_ijk", shapes[2], 0)
+        pcomp = None
+    else:
+        raw = np.asarray(probe_ijk, np.int64).reshape(-1, 3)
+        pcomp = np.ascontiguousarray(np.asarray(probe_comp, np.int64).reshape(-1), np.int32)
+        if pcomp.shape[0] != raw.shape[0] or np.any((pcomp < 0) | (pcomp > 2)):
+            raise ValueError("probe_comp needs one E component (0, 1 or 2) per probe")
+        hi = np.array([shapes[c] for c in range(3)])[pcomp] - 1
+        if raw.size and (np.any(raw < 0) or np.any(raw > hi)):
+            raise ValueError("a probe lies outside its component's grid")
+        probe_idx = np.ascontiguousarray(raw, np.int32)
     out_probe = torch.empty((n_steps, probe_idx.shape[0]), dtype=fdt, device=dev)
     out_v = torch.empty(n_steps, dtype=fdt, device=dev) if has_port else None
     out_i = torch.empty(n_steps, dtype=fdt, device=dev) if has_port else None
@@ -396,6 +424,8 @@ def simulate_3d(
         arr = chans[key][0]
         setattr(pts, key, arr.ctypes.data_as(_native.P_i32) if arr.shape[0] else None)
     pts.probe = probe_idx.ctypes.data_as(_native.P_i32) if probe_idx.shape[0] else None
+    pts.probe_comp = (pcomp.ctypes.data_as(_native.P_i32)
+                      if pcomp is not None and pcomp.shape[0] else None)
     if has_port:
         pts.port[0], pts.port[1], pts.port[2] = (int(v) for v in pidx)
     mon_arr = (_native.DftMonitor * max(len(mons), 1))()
@@ -427,6 +457,20 @@ def simulate_3d(
                                              ctypes.byref(nbytes)))
     ws = torch.empty(max(int(nbytes.value), 1), dtype=torch.uint8, device=dev)
     bufs.workspace, bufs.workspace_bytes = ws.data_ptr(), int(nbytes.value)
+    state_out = None
+    if state_in is not None or return_state:
+        sbytes = ctypes.c_size_t(0)
+        _native.check(lib.gdn_yee_state_size(ctypes.byref(prm), int(f64), ctypes.byref(sbytes)))
+        if state_in is not None:
+            if (not isinstance(state_in, torch.Tensor) or state_in.dtype != torch.uint8
+                    or state_in.numel() != int(sbytes.value) or state_in.device != ws.device
+                    or not state_in.is_contiguous()):
+                raise ValueError("state_in must be the contiguous uint8 device state of a run "
+                                 f"on this grid and dtype ({int(sbytes.value)} bytes)")
+            bufs.state_in = state_in.data_ptr()
+        if return_state:
+            state_out = torch.empty(int(sbytes.value), dtype=torch.uint8, device=dev)
+            bufs.state_out = state_out.data_ptr()
     stream = torch.cuda.current_stream(dev)
     run = lib.gdn_yee_run_f64 if f64 else lib.gdn_yee_run_f32
     with torch.cuda.device(dev):
@@ -444,4 +488,4 @@ def simulate_3d(
             dft = DFTMonitor(ft, *mon_out)
         else:
             dft = RegionDFTMonitor(ft, regions, *mon_out)
-    return SimResult3D(out_probe, out_v, out_i, out_e, dft, *fields, monitors)
+    return SimResult3D(out_probe, out_v, out_i, out_e, dft, *fields, monitors, state_out)

@@ -125,6 +125,32 @@ def simulate_3d_freq(grid: Grid3D, *, design_sigma=None, design_eps_r=None, desi
     return FreqPhasors3D(d.ex, d.ey, d.ez, d.hx, d.hy, d.hz, port_v, port_i)
 
 
+def _objective_boxes(grid, objective_kind, *, port_ijk=None, box_margin=None,
+                     monitor_region=None):
+    """DFT monitor boxes (comp, lo, hi) of what an objective reads:
+    objective_kind "port", "ntff_box" or "field", or a tuple of them."""
+    shapes = dr.full_field_shapes(grid.nx, grid.ny, grid.nz)
+    kinds = (objective_kind,) if isinstance(objective_kind, str) else tuple(objective_kind)
+    boxes = []
+    for kind in kinds:
+        if kind == "port":
+            if port_ijk is None:
+                raise ValueError("objective_kind='port' requires port_ijk")
+            boxes += dr.region_boxes(dr.port_regions(port_ijk, shapes))
+        elif kind == "ntff_box":
+            if box_margin is None:
+                raise ValueError("objective_kind='ntff_box' requires box_margin")
+            boxes += dr.ntff_face_boxes(grid, box_margin)
+        elif kind == "field":
+            if monitor_region is None:
+                raise ValueError("objective_kind='field' requires monitor_region")
+            boxes += dr.region_boxes(dr.field_regions(monitor_region, shapes))
+        else:
+            raise ValueError("objective_kind must be 'port', 'ntff_box' or 'field' (or a "
+                             f"tuple of them), got {kind!r}")
+    return boxes
+
+
 def _adjoint_channels(grid, cot):
     """Adjoint source cells and CW weights per channel (freq_adjoint.py:774-822).
 
@@ -224,25 +250,10 @@ def freq_adjoint_gradient_3d(grid: Grid3D, objective, *, design_sigma=None, desi
     # contraction see zero-filled full grids, so the gradient is unchanged.
     fwd_boxes = adj_boxes = None
     if objective_kind is not None:
-        kinds = (objective_kind,) if isinstance(objective_kind, str) else tuple(objective_kind)
         adj_boxes = dr.region_boxes(dr.design_region_to_slabs(design_region, shapes))
-        fwd_boxes = list(adj_boxes)
-        for kind in kinds:
-            if kind == "port":
-                if port_ijk is None:
-                    raise ValueError("objective_kind='port' requires port_ijk")
-                fwd_boxes += dr.region_boxes(dr.port_regions(port_ijk, shapes))
-            elif kind == "ntff_box":
-                if box_margin is None:
-                    raise ValueError("objective_kind='ntff_box' requires box_margin")
-                fwd_boxes += dr.ntff_face_boxes(grid, box_margin)
-            elif kind == "field":
-                if monitor_region is None:
-                    raise ValueError("objective_kind='field' requires monitor_region")
-                fwd_boxes += dr.region_boxes(dr.field_regions(monitor_region, shapes))
-            else:
-                raise ValueError("objective_kind must be 'port', 'ntff_box' or 'field' (or a "
-                                 f"tuple of them), got {kind!r}")
+        fwd_boxes = list(adj_boxes) + _objective_boxes(grid, objective_kind, port_ijk=port_ijk,
+                                                       box_margin=box_margin,
+                                                       monitor_region=monitor_region)
 
     def phasors(res, boxes):
         if boxes is None:

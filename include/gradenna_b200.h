@@ -242,7 +242,7 @@ typedef struct GdnYeeParams {
   int32_t npml, n_steps;
   int32_t n_src, n_jx, n_jy;      /* Jz (Ez edges), Jx (Ex), Jy (Ey) sources  */
   int32_t n_mx, n_my, n_mz;       /* magnetic currents on Hx, Hy, Hz          */
-  int32_t n_probes;               /* Ez probes                                */
+  int32_t n_probes;               /* E probes (Ez unless probe_comp is given)  */
   int32_t has_port;               /* 1: one z-directed RVS port               */
   int32_t n_freq, dft_f64, n_monitors;
   int32_t record_energy, cw_sources;
@@ -250,11 +250,15 @@ typedef struct GdnYeeParams {
 } GdnYeeParams;
 
 /* Host-memory index lists: (n, 3) int32 row-major (i, j, k) in each source's
- * own component grid; monitors as for 2D with comp 0..5 = ex ey ez hx hy hz. */
+ * own component grid; monitors as for 2D with comp 0..5 = ex ey ez hx hy hz.
+ * probe_comp (n_probes values, 0 = Ex, 1 = Ey, 2 = Ez; NULL = every probe on
+ * Ez, the reference's probe_ijk) picks the E component each probe records
+ * after the E half step; a probe lies on its own component's grid. */
 typedef struct GdnYeePoints {
   const int32_t *src, *jx, *jy, *mx, *my, *mz, *probe;
   int32_t port[3];
   const GdnDftMonitor* monitors;
+  const int32_t* probe_comp;
 } GdnYeePoints;
 
 /* Device buffers (field dtype float for *_f32, double for *_f64). The CPML
@@ -281,9 +285,23 @@ typedef struct GdnYeeBuffers {
   void *dft[6];                           /* full-grid DFT when n_monitors = 0 */
   void *workspace;
   size_t workspace_bytes;
+  /* Resumable runs (NULL = start from rest / keep nothing): the complete
+   * time-stepping state, the six fields and the twelve CPML psi arrays, as an
+   * opaque DEVICE blob of gdn_yee_state_size bytes. state_in is the state
+   * the run starts from (the final state of an earlier run on the same grid,
+   * CPML and dtype); state_out receives the state after the last step. Every
+   * per-step input (currents, port_vs, cw_env, ph_e, ph_h) is indexed by the
+   * run's own step counter, so a run resumed at absolute step s takes the
+   * rows s, s+1, ... of the whole run's tables, and its DFT outputs are the
+   * partial sums over its own steps. */
+  const void* state_in;
+  void* state_out;
 } GdnYeeBuffers;
 
 int gdn_yee_workspace_size(const GdnYeeParams* p, const GdnYeePoints* pts, int f64, size_t* bytes);
+
+/* Bytes of the resumable state blob of a grid (see GdnYeeBuffers.state_in). */
+int gdn_yee_state_size(const GdnYeeParams* p, int f64, size_t* bytes);
 
 /* Run the whole 3D time loop (replaces gradenna_3d_run_f32/_f64,
  * rust/src/lib3d.rs:191-828; step semantics of fdtd3d.py:559-679). */

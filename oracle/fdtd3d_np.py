@@ -10,6 +10,12 @@ energy. Field shapes (fdtd3d.py:1-13):
     Ex (nx-1, ny, nz)   Ey (nx, ny-1, nz)   Ez (nx, ny, nz-1)
     Hx (nx, ny-1, nz-1) Hy (nx-1, ny, nz-1) Hz (nx-1, ny-1, nz)
 
+Test conveniences beyond the reference's interface (the algorithm is
+unchanged): ``probe_comp`` records Ex / Ey / Ez probes, and ``state_in`` /
+``return_state`` / ``step0`` resume a run from an earlier run's state (six
+fields and twelve psi pairs) with the DFT phases of the absolute steps, so
+that checkpointed gradient logic can be checked on the CPU.
+
 Only tests and CPU-baseline code may import this module.
 """
 
@@ -59,6 +65,7 @@ class SimResult3D(NamedTuple):
     hx: np.ndarray
     hy: np.ndarray
     hz: np.ndarray
+    state: tuple | None = None
 
 
 def full_shapes(nx, ny, nz):
@@ -72,7 +79,8 @@ def simulate_3d(grid: Grid3D, *, eps_r=1.0, sigma=0.0, source_ijk=None, source_c
                 source_y_current=None, mx_ijk=None, mx_current=None, my_ijk=None,
                 my_current=None, mz_ijk=None, mz_current=None, port_ijk=None,
                 port_voltage=None, port_resistance=50.0, probe_ijk=(), cpml=CPMLSpec(),
-                dft_freqs=None, dft_regions=None, record_energy=False, dtype=np.float64):
+                dft_freqs=None, dft_regions=None, record_energy=False, dtype=np.float64,
+                probe_comp=None, state_in=None, return_state=False, step0=0):
     """fdtd3d.py:258-770 restated; dft_regions: dict comp -> (lo, hi) boxes."""
     dtype = np.dtype(dtype)
     f = dtype.type
@@ -150,7 +158,7 @@ def simulate_3d(grid: Grid3D, *, eps_r=1.0, sigma=0.0, source_ijk=None, source_c
     if has_dft:
         fr = np.atleast_1d(np.asarray(dft_freqs, np.float64))
         cdtype = np.result_type(dtype, np.complex64)
-        nn = np.arange(n_steps, dtype=np.float64)
+        nn = np.arange(step0, step0 + n_steps, dtype=np.float64)
         e_phase = (dt * np.exp(-2j * np.pi * np.outer(nn + 1.0, fr) * dt)).astype(cdtype)
         h_phase = (dt * np.exp(-2j * np.pi * np.outer(nn + 0.5, fr) * dt)).astype(cdtype)
         shapes = full_shapes(nx, ny, nz)
@@ -174,6 +182,9 @@ def simulate_3d(grid: Grid3D, *, eps_r=1.0, sigma=0.0, source_ijk=None, source_c
         hyx=pair((npml, ny, nz - 1)), hyz=pair((nx - 1, ny, npml)),
         hzx=pair((npml, ny - 1, nz)), hzy=pair((nx - 1, npml, nz)),
     )
+    if state_in is not None:
+        ex, ey, ez, hx, hy, hz = (a.copy() for a in state_in[:6])
+        psi = {k: tuple(a.copy() for a in v) for k, v in state_in[6].items()}
     probe_out = np.zeros((n_steps, probe_idx.shape[0]), dtype)
     v_out = np.zeros(n_steps, dtype)
     i_out = np.zeros(n_steps, dtype)
@@ -246,7 +257,11 @@ def simulate_3d(grid: Grid3D, *, eps_r=1.0, sigma=0.0, source_ijk=None, source_c
                 ph = e_phase[n] if k[0] == "e" else h_phase[n]
                 patch = fields[k][lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]]
                 a += ph[:, None, None, None] * patch[None]
-        probe_out[n] = ez[probe_idx[:, 0], probe_idx[:, 1], probe_idx[:, 2]]
+        if probe_comp is None:
+            probe_out[n] = ez[probe_idx[:, 0], probe_idx[:, 1], probe_idx[:, 2]]
+        else:
+            for q, (pc, (a, b, c)) in enumerate(zip(probe_comp, probe_idx)):
+                probe_out[n, q] = (ex, ey, ez)[pc][a, b, c]
         if has_port:
             v_out[n] = f(-0.5) * f(dz) * (ez_prev[pi, pj, pk] + ez[pi, pj, pk])
             i_out[n] = i_loop
@@ -258,7 +273,8 @@ def simulate_3d(grid: Grid3D, *, eps_r=1.0, sigma=0.0, source_ijk=None, source_c
             energy[n] = ue + uh
 
     return SimResult3D(probe_out, v_out if has_port else None, i_out if has_port else None,
-                       energy, acc if has_dft else None, ex, ey, ez, hx, hy, hz)
+                       energy, acc if has_dft else None, ex, ey, ez, hx, hy, hz,
+                       (ex, ey, ez, hx, hy, hz, psi) if return_state else None)
 
 
 def time_series_dft(x, dt, freqs, t0=0.0):
