@@ -76,12 +76,12 @@ struct Dev3 {
   long long mon_cells;
   int n_mons;
   const Mon3* mons;
-  // Monitor cells split by field kind for the ring gathers: side 0 = E
-  // components, 1 = H; gmon[side] lists that side's monitors, gcum[side] the
-  // running count of their cells (gn[side] + 1 entries).
-  const int* gmon[2];
-  const long long* gcum[2];
-  int gn[2];
+  // Ring gathers: the ring holds the E-side monitors' cells first (gcells[0]
+  // of them), then the H-side ones (gcells[1]); gsrc[r] is the offset of
+  // ring cell r's field value in the contiguous block of the six fields
+  // (32-bit when the block holds fewer than 2^32 values, else gsrc64).
+  const unsigned* gsrc;
+  const long long* gsrc64;
   long long gcells[2];
   const unsigned char* cls;  // per plane-box work flags (F_*)
   T* cwv;                // CW source values of the chunk: [sub][cw_off[type] + m]
@@ -148,47 +148,26 @@ __global__ void __launch_bounds__(256) yee_cw_synth(Dev3<T> d, int cnt) {
 
 // Monitor ring writes of step n (fdtd3d.py:635-662, the running DFT's
 // samples): after the H (side 1) or the E (side 0) half step, one thread per
-// monitored cell of that side copies the field value into ring slot n % R.
+// monitored cell of that side copies the field value into ring slot n % R,
+// through a table of field offsets built once on the host.
 // Doing this in its own launch keeps the per-cell stencil kernels free of
 // monitor bookkeeping; the ring traffic is O(monitored cells).
 template <typename T>
 __global__ void __launch_bounds__(256) yee_gather(Dev3<T> d, int sub, int side) {
-  const long long r0 = (long long)blockIdx.x * blockDim.x;
-  const long long r = r0 + threadIdx.x;
-  const long long* cum = d.gcum[side];
-  // The block's first monitor (one search per block; a block spans few
-  // monitors), then each thread steps forward to its own.
-  __shared__ int s_lo;
-  if (threadIdx.x == 0) {
-    int lo = 0, hi = d.gn[side] - 1;
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (cum[mid] <= r0)
-        lo = mid;
-      else
-        hi = mid - 1;
-    }
-    s_lo = lo;
-  }
-  __syncthreads();
+  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= d.gcells[side]) return;
-  int q = s_lo;
-  while (cum[q + 1] <= r) ++q;
-  const Mon3 m = d.mons[d.gmon[side][q]];
-  const int loc = int(r - cum[q]);  // a monitor box holds fewer than 2^31 cells
-  const int k = loc % m.s2, t = loc / m.s2;
-  const int j = t % m.s1, i = t / m.s1;
+  const long long at_r = (side ? d.gcells[0] : 0) + r;
   const int n = *d.step_base + sub;
-  d.mring[(long long)(n % d.R) * d.mon_cells + m.off + loc] =
-      d.f[m.comp][at(d, m.lo0 + i, m.lo1 + j, m.lo2 + k)];
+  const long long src = d.gsrc ? (long long)d.gsrc[at_r] : d.gsrc64[at_r];
+  d.mring[(long long)(n % d.R) * d.mon_cells + at_r] = d.f[0][src];
 }
 
 // Per plane-box flags (bit set = the box needs that work), computed on the
 // host so that most boxes run the bare stencil with no per-thread checks.
 enum : unsigned char { F_HPTS = 1, F_EPTS = 2, F_CPML = 8 };
 
-// Planes per CTA: a CTA walks NI consecutive i-planes of its (j, k) tile.
-constexpr int NI = 8;
+// A CTA walks `ni` consecutive i-planes of its (j, k) tile (chosen on the
+// host, planes_per_cta).
 
 // CPML coefficients of sample s of axis ax (E-type: the ns = n-2 samples
 // of the PEC interior; H-type: the ns = n-1 half samples). Returns whether
@@ -237,54 +216,64 @@ __device__ __forceinline__ T psi_term(const Ax<T>& a, T diff, T& psi) {
 // A CTA covers a BJ x BK tile of NI consecutive i-planes.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(NT) yee_h(Dev3<T> d, int sub) {
+__global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 5 : 3) yee_h(Dev3<T> d, int sub, int ni) {
   const int n = *d.step_base + sub;
   const int k = blockIdx.x * BK + threadIdx.x;
   const int j = blockIdx.y * BJ + threadIdx.y;
   const int nx = d.nx, ny = d.ny, nz = d.nz;
   const bool live = j < ny && k < nz;
   const int tid = threadIdx.y * BK + threadIdx.x;
-  const int i1 = min(nx, int(blockIdx.z + 1) * NI);
-  long long c = at(d, int(blockIdx.z) * NI, j, k);
-  const long long di = (long long)d.sy * d.sz, dj = d.sz, vol = d.vol;
-  const T *ex = d.f[0], *ey = d.f[1], *ez = d.f[2];
+  const int i0 = int(blockIdx.z) * ni, i1 = min(nx, i0 + ni);
+  // 32-bit cell offsets (a padded volume holds fewer than 2^31 cells).
+  const int di = d.sy * d.sz, dj = d.sz;
+  int c = ((i0 + 1) * d.sy + (j + 1)) * d.sz + (k + 1);
+  const T* __restrict__ ex = d.f[0];
+  const T* __restrict__ ey = d.f[1];
+  const T* __restrict__ ez = d.f[2];
   T *hx = d.f[3], *hy = d.f[4], *hz = d.f[5];
-  T* P = d.psi;
+  T *pxz = d.psi + P_HXZ * d.vol, *pxy = d.psi + P_HXY * d.vol, *pyx = d.psi + P_HYX * d.vol,
+    *pyz = d.psi + P_HYZ * d.vol, *pzy = d.psi + P_HZY * d.vol, *pzx = d.psi + P_HZX * d.vol;
   const T dt_mu = d.dt_mu, idx = d.inv_d[0], idy = d.inv_d[1], idz = d.inv_d[2];
   // This thread's y and z CPML samples (H-type) are fixed over the planes.
   Ax<T> ay, az;
   ay.on = slab_coef<T, false>(d, 1, j, ny - 1, ay.b, ay.c, ay.ik);
   az.on = slab_coef<T, false>(d, 2, k, nz - 1, az.b, az.c, az.ik);
-  for (int i = blockIdx.z * NI; i < i1; ++i, c += di) {
+  const bool vx = j < ny - 1 && k < nz - 1, kin = k < nz - 1, jin = j < ny - 1;
+  // Ey and Ez of plane i + 1 become plane i + 1's own values next iteration.
+  T ey0 = T(0), ez0 = T(0);
+  if (live) {
+    ey0 = ey[c];
+    ez0 = ez[c];
+  }
+  for (int i = i0; i < i1; ++i, c += di) {
     const int cta = (i * d.gj + blockIdx.y) * d.gk + blockIdx.x;
     const unsigned fl = d.cls[cta];
     if (live) {
       Ax<T> ax;
       ax.on = slab_coef<T, false>(d, 0, i, nx - 1, ax.b, ax.c, ax.ik);
       // Every operand first (all in the padded volumes), then the updates.
-      const T ex0 = ex[c], ey0 = ey[c], ez0 = ez[c];
+      const T ex0 = ex[c];
       const T eyk = ey[c + 1], ezj = ez[c + dj], ezi = ez[c + di];
       const T exk = ex[c + 1], exj = ex[c + dj], eyi = ey[c + di];
       const T hx0 = hx[c], hy0 = hy[c], hz0 = hz[c];
-      const bool vx = j < ny - 1 && k < nz - 1, vy = i < nx - 1 && k < nz - 1,
-                 vz = i < nx - 1 && j < ny - 1;
+      const bool vy = i < nx - 1 && kin, vz = i < nx - 1 && jin;
       T p_xz = T(0), p_xy = T(0), p_yx = T(0), p_yz = T(0), p_zy = T(0), p_zx = T(0);
-      if (vx && az.on) p_xz = P[P_HXZ * vol + c];
-      if (vx && ay.on) p_xy = P[P_HXY * vol + c];
-      if (vy && ax.on) p_yx = P[P_HYX * vol + c];
-      if (vy && az.on) p_yz = P[P_HYZ * vol + c];
-      if (vz && ay.on) p_zy = P[P_HZY * vol + c];
-      if (vz && ax.on) p_zx = P[P_HZX * vol + c];
+      if (vx && az.on) p_xz = pxz[c];
+      if (vx && ay.on) p_xy = pxy[c];
+      if (vy && ax.on) p_yx = pyx[c];
+      if (vy && az.on) p_yz = pyz[c];
+      if (vz && ay.on) p_zy = pzy[c];
+      if (vz && ax.on) p_zx = pzx[c];
       if (vx) {  // Hx (nx, ny-1, nz-1): +dt/mu (t_hxz - t_hxy)
         const T dey_dz = (eyk - ey0) * idz, dez_dy = (ezj - ez0) * idy;
         T tz = dey_dz, ty = dez_dy;
         if (az.on) {
           tz = psi_term(az, dey_dz, p_xz);
-          P[P_HXZ * vol + c] = p_xz;
+          pxz[c] = p_xz;
         }
         if (ay.on) {
           ty = psi_term(ay, dez_dy, p_xy);
-          P[P_HXY * vol + c] = p_xy;
+          pxy[c] = p_xy;
         }
         hx[c] = hx0 + dt_mu * (tz - ty);
       }
@@ -293,11 +282,11 @@ __global__ void __launch_bounds__(NT) yee_h(Dev3<T> d, int sub) {
         T tx = dez_dx, tz = dex_dz;
         if (ax.on) {
           tx = psi_term(ax, dez_dx, p_yx);
-          P[P_HYX * vol + c] = p_yx;
+          pyx[c] = p_yx;
         }
         if (az.on) {
           tz = psi_term(az, dex_dz, p_yz);
-          P[P_HYZ * vol + c] = p_yz;
+          pyz[c] = p_yz;
         }
         hy[c] = hy0 + dt_mu * (tx - tz);
       }
@@ -306,14 +295,16 @@ __global__ void __launch_bounds__(NT) yee_h(Dev3<T> d, int sub) {
         T ty = dex_dy, tx = dey_dx;
         if (ay.on) {
           ty = psi_term(ay, dex_dy, p_zy);
-          P[P_HZY * vol + c] = p_zy;
+          pzy[c] = p_zy;
         }
         if (ax.on) {
           tx = psi_term(ax, dey_dx, p_zx);
-          P[P_HZX * vol + c] = p_zx;
+          pzx[c] = p_zx;
         }
         hz[c] = hz0 + dt_mu * (ty - tx);
       }
+      ey0 = eyi;
+      ez0 = ezi;
     }
     if (fl & F_HPTS) {
       __syncthreads();
@@ -334,7 +325,7 @@ __global__ void __launch_bounds__(NT) yee_h(Dev3<T> d, int sub) {
 // probes, V/I and E monitors. Same CTA geometry as yee_h.
 // ---------------------------------------------------------------------------
 template <typename T>
-__global__ void __launch_bounds__(NT) yee_e(Dev3<T> d, int sub) {
+__global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 5 : 3) yee_e(Dev3<T> d, int sub, int ni) {
   __shared__ T s_port[3];  // Ez^n, curl_z and the plain-updated Ez at the port edge
   const int n = *d.step_base + sub;
   const int k = blockIdx.x * BK + threadIdx.x;
@@ -342,50 +333,60 @@ __global__ void __launch_bounds__(NT) yee_e(Dev3<T> d, int sub) {
   const int nx = d.nx, ny = d.ny, nz = d.nz;
   const bool live = j < ny && k < nz;
   const int tid = threadIdx.y * BK + threadIdx.x;
-  const int i1 = min(nx, int(blockIdx.z + 1) * NI);
-  long long c = at(d, int(blockIdx.z) * NI, j, k);
-  const long long di = (long long)d.sy * d.sz, dj = d.sz, vol = d.vol;
+  const int i0 = int(blockIdx.z) * ni, i1 = min(nx, i0 + ni);
+  const int di = d.sy * d.sz, dj = d.sz;
+  int c = ((i0 + 1) * d.sy + (j + 1)) * d.sz + (k + 1);
+  long long g = ((long long)i0 * ny + j) * nz + k;  // node coefficients
+  const long long dgi = (long long)ny * nz;
   T *ex = d.f[0], *ey = d.f[1], *ez = d.f[2];
-  const T *hx = d.f[3], *hy = d.f[4], *hz = d.f[5];
-  T* P = d.psi;
+  const T* __restrict__ hx = d.f[3];
+  const T* __restrict__ hy = d.f[4];
+  const T* __restrict__ hz = d.f[5];
+  T *pxy = d.psi + P_EXY * d.vol, *pxz = d.psi + P_EXZ * d.vol, *pyz = d.psi + P_EYZ * d.vol,
+    *pyx = d.psi + P_EYX * d.vol, *pzx = d.psi + P_EZX * d.vol, *pzy = d.psi + P_EZY * d.vol;
   const T idx = d.inv_d[0], idy = d.inv_d[1], idz = d.inv_d[2];
   // E-type samples of this thread's y and z (the PEC interior, node - 1).
   Ax<T> ay, az;
   ay.on = slab_coef<T, true>(d, 1, j - 1, ny - 2, ay.b, ay.c, ay.ik);
   az.on = slab_coef<T, true>(d, 2, k - 1, nz - 2, az.b, az.c, az.ik);
-  for (int i = blockIdx.z * NI; i < i1; ++i, c += di) {
+  const bool jx = j >= 1 && j <= ny - 2, kx = k >= 1 && k <= nz - 2;
+  const bool vx_jk = jx && kx, vy_jk = j < ny - 1 && kx, vz_jk = jx && k < nz - 1;
+  // Hy and Hz of plane i - 1 (the previous plane's own values).
+  T hyi = T(0), hzi = T(0);
+  if (live) {
+    hyi = hy[c - di];
+    hzi = hz[c - di];
+  }
+  for (int i = i0; i < i1; ++i, c += di, g += dgi) {
     const int cta = (i * d.gj + blockIdx.y) * d.gk + blockIdx.x;
     const unsigned fl = d.cls[cta];
     const bool port_here = d.has_port && cta == d.port_cta;
     if (live) {
       Ax<T> ax;
       ax.on = slab_coef<T, true>(d, 0, i - 1, nx - 2, ax.b, ax.c, ax.ik);
-      const long long g = ((long long)i * ny + j) * nz + k;  // node coefficients
       const T hx0 = hx[c], hy0 = hy[c], hz0 = hz[c];
-      const T hzj = hz[c - dj], hyk = hy[c - 1], hxk = hx[c - 1];
-      const T hzi = hz[c - di], hyi = hy[c - di], hxj = hx[c - dj];
+      const T hzj = hz[c - dj], hyk = hy[c - 1], hxk = hx[c - 1], hxj = hx[c - dj];
       const T ex0 = ex[c], ey0 = ey[c], ez0 = ez[c];
       const T ca = d.ca[g], cb = d.cb[g];
-      const bool vx = i < nx - 1 && j >= 1 && j <= ny - 2 && k >= 1 && k <= nz - 2;
-      const bool vy = i >= 1 && i <= nx - 2 && j < ny - 1 && k >= 1 && k <= nz - 2;
-      const bool vz = i >= 1 && i <= nx - 2 && j >= 1 && j <= ny - 2 && k < nz - 1;
+      const bool iin = i >= 1 && i <= nx - 2;
+      const bool vx = i < nx - 1 && vx_jk, vy = iin && vy_jk, vz = iin && vz_jk;
       T p_xy = T(0), p_xz = T(0), p_yz = T(0), p_yx = T(0), p_zx = T(0), p_zy = T(0);
-      if (vx && ay.on) p_xy = P[P_EXY * vol + c];
-      if (vx && az.on) p_xz = P[P_EXZ * vol + c];
-      if (vy && az.on) p_yz = P[P_EYZ * vol + c];
-      if (vy && ax.on) p_yx = P[P_EYX * vol + c];
-      if (vz && ax.on) p_zx = P[P_EZX * vol + c];
-      if (vz && ay.on) p_zy = P[P_EZY * vol + c];
+      if (vx && ay.on) p_xy = pxy[c];
+      if (vx && az.on) p_xz = pxz[c];
+      if (vy && az.on) p_yz = pyz[c];
+      if (vy && ax.on) p_yx = pyx[c];
+      if (vz && ax.on) p_zx = pzx[c];
+      if (vz && ay.on) p_zy = pzy[c];
       if (vx) {  // Ex (nx-1, ny, nz) interior j, k: t_exy - t_exz
         const T dhz_dy = (hz0 - hzj) * idy, dhy_dz = (hy0 - hyk) * idz;
         T ty = dhz_dy, tz = dhy_dz;
         if (ay.on) {
           ty = psi_term(ay, dhz_dy, p_xy);
-          P[P_EXY * vol + c] = p_xy;
+          pxy[c] = p_xy;
         }
         if (az.on) {
           tz = psi_term(az, dhy_dz, p_xz);
-          P[P_EXZ * vol + c] = p_xz;
+          pxz[c] = p_xz;
         }
         ex[c] = ca * ex0 + cb * (ty - tz);
       }
@@ -394,11 +395,11 @@ __global__ void __launch_bounds__(NT) yee_e(Dev3<T> d, int sub) {
         T tz = dhx_dz, tx = dhz_dx;
         if (az.on) {
           tz = psi_term(az, dhx_dz, p_yz);
-          P[P_EYZ * vol + c] = p_yz;
+          pyz[c] = p_yz;
         }
         if (ax.on) {
           tx = psi_term(ax, dhz_dx, p_yx);
-          P[P_EYX * vol + c] = p_yx;
+          pyx[c] = p_yx;
         }
         ey[c] = ca * ey0 + cb * (tz - tx);
       }
@@ -407,11 +408,11 @@ __global__ void __launch_bounds__(NT) yee_e(Dev3<T> d, int sub) {
         T tx = dhy_dx, ty = dhx_dy;
         if (ax.on) {
           tx = psi_term(ax, dhy_dx, p_zx);
-          P[P_EZX * vol + c] = p_zx;
+          pzx[c] = p_zx;
         }
         if (ay.on) {
           ty = psi_term(ay, dhx_dy, p_zy);
-          P[P_EZY * vol + c] = p_zy;
+          pzy[c] = p_zy;
         }
         const T curl = tx - ty;
         const T upd = ca * ez0 + cb * curl;
@@ -422,6 +423,8 @@ __global__ void __launch_bounds__(NT) yee_e(Dev3<T> d, int sub) {
         }
         ez[c] = upd;
       }
+      hyi = hy0;
+      hzi = hz0;
     }
     if (fl & F_EPTS) {
       __syncthreads();
@@ -631,8 +634,8 @@ static void comp_shape(int c, int nx, int ny, int nz, int s[3]) {
 struct Layout3 {
   int sy = 0, sz = 0, gj = 0, gk = 0, n_cta = 0, R = 32;
   long long vol = 0, mon_cells = 0;
-  size_t fields, psi, zero_end, off[7], pts[7], pcomp, mons, gmon, gcum, mring, step, eacc, cwv,
-      cls, total;
+  size_t fields, psi, zero_end, off[7], pts[7], pcomp, mons, gsrc, mring, step, eacc, cwv, cls,
+      total;
 };
 
 // Monitor boxes {comp, lo0, lo1, lo2, s0, s1, s2} in ring order: the listed
@@ -707,9 +710,7 @@ static Layout3 make_layout3(const GdnYeeParams* p, const GdnYeePoints* pts, size
   }
   L.pcomp = cv.take<int>(std::max(p->n_probes, 1));
   L.mons = cv.take<Mon3>(std::max(p->n_monitors, 6));
-  const int nmon = std::max(p->n_monitors, 6);
-  L.gmon = cv.take<int>(2 * size_t(nmon));
-  L.gcum = cv.take<long long>(2 * size_t(nmon + 1));
+  L.gsrc = cv.take<long long>(std::max<size_t>(size_t(L.mon_cells), 1));
   L.mring = cv.take<char>(std::max<size_t>(size_t(L.mon_cells) * L.R, 1) * esize);
   L.eacc = cv.take<double>(p->record_energy ? 2 * size_t(std::max(p->n_steps, 1)) : 1);
   long long cw_total = 0;
@@ -799,6 +800,20 @@ static int validate3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYe
   if ((p->n_src && !b->cb_src) || (p->n_jx && !b->cb_jx) || (p->n_jy && !b->cb_jy))
     GDN_BAD_ARG("source coefficients are null");
   if (p->dt <= 0 || p->dx <= 0 || p->dy <= 0 || p->dz <= 0) GDN_BAD_ARG("dt, dx, dy, dz must be positive");
+  return GDN_OK;
+}
+
+// Planes per CTA for a step kernel: the CTAs of `cols` (j, k) tile columns
+// split the nx planes so that the whole grid is one wave of resident CTAs.
+template <typename K>
+static int planes_per_cta(K kernel, int nx, int cols, int* ni) {
+  int dev = 0, sms = 0, per_sm = 0;
+  GDN_TRY_CUDA(cudaGetDevice(&dev));
+  GDN_TRY_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  GDN_TRY_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, NT, 0));
+  const long long slots = (long long)std::max(sms, 1) * std::max(per_sm, 1);
+  const long long per_col = std::max<long long>(1, slots / std::max(cols, 1));
+  *ni = int(std::max<long long>(1, div_up(nx, per_col)));
   return GDN_OK;
 }
 
@@ -948,31 +963,44 @@ static int run3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuff
       ++k;
     }
   }
-  // Gather tables: the E-side and the H-side monitors with running cell counts.
+  // Ring order: the E-side monitors' cells, then the H-side ones (the fold
+  // finds a cell's monitor by binary search over the offsets, so the list
+  // is reordered the same way), and the gather table of field offsets.
   {
-    const int nmon = std::max(p->n_monitors, 6);
-    std::vector<int> gm(2 * size_t(nmon), 0);
-    std::vector<long long> gc(2 * size_t(nmon + 1), 0);
-    for (int side = 0; side < 2; ++side) {
-      int q = 0;
-      long long cum = 0;
-      for (int mi = 0; mi < int(mons.size()); ++mi) {
-        if ((mons[mi].comp >= 3) != (side == 1) || mons[mi].count <= 0) continue;
-        gm[side * nmon + q] = mi;
-        gc[side * (nmon + 1) + q] = cum;
-        cum += mons[mi].count;
-        ++q;
-      }
-      gc[side * (nmon + 1) + q] = cum;
-      d.gn[side] = q;
-      d.gcells[side] = cum;
-      d.gmon[side] = reinterpret_cast<const int*>(ws + L.gmon) + side * nmon;
-      d.gcum[side] = reinterpret_cast<const long long*>(ws + L.gcum) + side * (nmon + 1);
+    std::stable_partition(mons.begin(), mons.end(), [](const Mon3& m) { return m.comp < 3; });
+    long long off = 0;
+    d.gcells[0] = d.gcells[1] = 0;
+    for (Mon3& m : mons) {
+      m.off = off;
+      off += m.count;
+      d.gcells[m.comp >= 3] += m.count;
     }
-    GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.gmon, gm.data(), gm.size() * sizeof(int),
-                                 cudaMemcpyHostToDevice, stream));
-    GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.gcum, gc.data(), gc.size() * sizeof(long long),
-                                 cudaMemcpyHostToDevice, stream));
+    std::vector<long long> src(std::max<long long>(L.mon_cells, 1));
+    const bool narrow = (long long)NC * L.vol < (1LL << 32);
+    for (const Mon3& m : mons) {
+      long long r = m.off;
+      for (int i = 0; i < m.s0; ++i)
+        for (int j = 0; j < m.s1; ++j) {
+          const long long row = (long long)m.comp * L.vol +
+                                 ((long long)(m.lo0 + i + 1) * L.sy + (m.lo1 + j + 1)) * L.sz +
+                                 (m.lo2 + 1);
+          for (int k = 0; k < m.s2; ++k) src[r++] = row + k;
+        }
+    }
+    d.gsrc = nullptr;
+    d.gsrc64 = nullptr;
+    if (narrow) {
+      std::vector<unsigned> s32(src.begin(), src.end());
+      if (L.mon_cells > 0)
+        GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.gsrc, s32.data(), size_t(L.mon_cells) * sizeof(unsigned),
+                                     cudaMemcpyHostToDevice, stream));
+      d.gsrc = reinterpret_cast<const unsigned*>(ws + L.gsrc);
+    } else {
+      if (L.mon_cells > 0)
+        GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.gsrc, src.data(), size_t(L.mon_cells) * sizeof(long long),
+                                     cudaMemcpyHostToDevice, stream));
+      d.gsrc64 = reinterpret_cast<const long long*>(ws + L.gsrc);
+    }
   }
   d.n_mons = int(mons.size());
   d.mons = reinterpret_cast<const Mon3*>(ws + L.mons);
@@ -1028,7 +1056,13 @@ static int run3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuff
     GDN_TRY_CUDA(cudaMemsetAsync(eacc, 0, 2 * size_t(std::max(N, 1)) * sizeof(double), stream));
 
   const dim3 blk(BK, BJ);
-  const dim3 grd(L.gk, L.gj, unsigned(div_up(nx, NI)));
+  // Planes per CTA: the fewest that fit every CTA of the grid into one wave
+  // of resident CTAs (a partial second wave would idle most SMs).
+  int ni_h = 0, ni_e = 0;
+  if ((st = planes_per_cta(yee_h<T>, nx, L.gj * L.gk, &ni_h))) return st;
+  if ((st = planes_per_cta(yee_e<T>, nx, L.gj * L.gk, &ni_e))) return st;
+  const dim3 grd_h(L.gk, L.gj, unsigned(div_up(nx, ni_h)));
+  const dim3 grd_e(L.gk, L.gj, unsigned(div_up(nx, ni_e)));
   const int eblocks = int(std::min<long long>(div_up((long long)nx * ny * nz, 256), 148 * 8));
   auto enqueue = [&](int cnt, cudaStream_t s) -> uint64_t {
     uint64_t k = 0;
@@ -1039,13 +1073,13 @@ static int run3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuff
     }
     const unsigned gb0 = unsigned(div_up(d.gcells[0], 256)), gb1 = unsigned(div_up(d.gcells[1], 256));
     for (int t = 0; t < cnt; ++t) {
-      yee_h<T><<<grd, blk, 0, s>>>(d, t);
+      yee_h<T><<<grd_h, blk, 0, s>>>(d, t, ni_h);
       k += 1;
       if (gb1 > 0) {
         yee_gather<T><<<gb1, 256, 0, s>>>(d, t, 1);
         ++k;
       }
-      yee_e<T><<<grd, blk, 0, s>>>(d, t);
+      yee_e<T><<<grd_e, blk, 0, s>>>(d, t, ni_e);
       k += 1;
       if (gb0 > 0) {
         yee_gather<T><<<gb0, 256, 0, s>>>(d, t, 0);
