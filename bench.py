@@ -276,16 +276,13 @@ def pop_cells(specs):
     return sum(sp["grid"].nx * sp["grid"].ny * len(sp["env"]) for sp in specs)
 
 
-def make_objective(grid, box):
-    from gradenna_b200.monitors import poynting_flux_box_2d
-    from gradenna_b200.sparams import s11_power_wave
+def make_objective(grid, box, port_ij):
+    """sum_k P_rad,k - sum_k |S11_k|^2 of port 0: the built-in objective, whose
+    value and adjoint weights come from one fused kernel on the forward
+    run's monitor boxes (gradenna_b200.objectives)."""
+    from gradenna_b200.objectives import RadiatedPowerS11
 
-    def obj(ph):
-        p = poynting_flux_box_2d(ph.dft_ez, ph.dft_hx, ph.dft_hy, grid, box)
-        s = s11_power_wave(ph.port_v[:, 0], ph.port_i[:, 0], RS)
-        return p.sum() - (s.real**2 + s.imag**2).sum()
-
-    return obj
+    return RadiatedPowerS11(grid, box, port_ij, FREQS, resistance=RS, w_prad=1.0, w_s11=-1.0)
 
 
 def monitors_for(w):
@@ -304,7 +301,8 @@ def gradient_call(w, sigma_dev, vs_dev, dtype, mons):
     grid = w["grid"]
     ports = (gb.Port(w["ports"][0], RS, vs_dev), gb.Port(w["ports"][1], RS, None))
     return freq_adjoint_gradient(
-        grid, make_objective(grid, w["box"]), design_sigma=sigma_dev, design_region=w["design"],
+        grid, make_objective(grid, w["box"], w["ports"][0]), design_sigma=sigma_dev,
+        design_region=w["design"],
         dft_freqs=FREQS, env=w["env"], ports=ports, cpml=gb.CPMLSpec(NPML), dtype=dtype,
         objective_monitors=mons)["sigma"]
 

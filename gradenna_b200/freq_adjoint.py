@@ -212,6 +212,28 @@ def _adjoint_sources(plan: _Plan, cot):
     return out
 
 
+def _fusable(plan: _Plan, objective):
+    """True when the objective has a fused device evaluation for this run:
+    its frequencies are the run's and the forward run recorded boxes."""
+    return (getattr(objective, "fused_tm", None) is not None
+            and plan.objective_monitors is not None
+            and tuple(getattr(objective, "freqs", ())) == plan.freqs)
+
+
+def _objective_sources(plan: _Plan, objective, fwd):
+    """(objective value, adjoint CW sources) of the forward run. An objective
+    with a fused device evaluation (gradenna_b200.objectives) takes one
+    kernel launch on the recorded monitor boxes; any other objective goes
+    through full-grid phasors and torch autograd."""
+    if _fusable(plan, objective):
+        val, _, _, lists = objective.fused_tm(list(plan.objective_monitors),
+                                              list(fwd.monitors[1:]), plan.device)
+        return val, [(idx, w) if len(idx) else (None, None) for idx, w in lists]
+    full = _scatter_full(plan, fwd)
+    val, cot = _cotangents(plan, objective, full, fwd)
+    return val, _adjoint_sources(plan, cot)
+
+
 def _adjoint_kwargs(plan: _Plan, eps_r, sigma, srcs):
     """simulate_tm keyword arguments of the adjoint run (None without sources)."""
     (a0, a1), (b0, b1) = plan.bounds
@@ -305,9 +327,8 @@ def freq_adjoint_gradient(grid: Grid2D, objective, *, design_sigma=None, design_
                       cpml, dtype, device, objective_monitors, exact)
     eps_r, sigma = _full_eps_sigma(grid, design_sigma, design_eps_r, design_region, plan.device)
     fwd = _forward(plan, eps_r, sigma)
-    full = _scatter_full(plan, fwd)
-    _, cot = _cotangents(plan, objective, full, fwd)
-    adj = _adjoint_run(plan, eps_r, sigma, _adjoint_sources(plan, cot))
+    _, srcs = _objective_sources(plan, objective, fwd)
+    adj = _adjoint_run(plan, eps_r, sigma, srcs)
     out = {}
     if adj is None:
         shp = tuple(b - a for a, b in plan.bounds)
@@ -337,18 +358,22 @@ class FreqAdjointObjective(torch.autograd.Function):
         eps_r, sigma = _full_eps_sigma(plan.grid, design_sigma, None, plan.design_region,
                                        plan.device)
         fwd = _forward(plan, eps_r, sigma)
-        full = _scatter_full(plan, fwd)
-        val = _objective_value(plan, objective, full, fwd)
+        if _fusable(plan, objective):
+            val, srcs = _objective_sources(plan, objective, fwd)
+        else:
+            srcs = None
+            val = _objective_value(plan, objective, _scatter_full(plan, fwd), fwd)
         ctx.plan, ctx.objective = plan, objective
-        ctx.state = (eps_r, sigma, fwd, full)
+        ctx.state = (eps_r, sigma, fwd, srcs)
         return val.detach().to(torch.float64)
 
     @staticmethod
     def backward(ctx, g):
         plan = ctx.plan
-        eps_r, sigma, fwd, full = ctx.state
-        _, cot = _cotangents(plan, ctx.objective, full, fwd)
-        adj = _adjoint_run(plan, eps_r, sigma, _adjoint_sources(plan, cot))
+        eps_r, sigma, fwd, srcs = ctx.state
+        if srcs is None:
+            _, srcs = _objective_sources(plan, ctx.objective, fwd)
+        adj = _adjoint_run(plan, eps_r, sigma, srcs)
         if adj is None:
             return torch.zeros_like(sigma[plan.design_region]), None, None
         gs, _ = _contract(plan, eps_r, sigma, fwd.monitors[0], adj.monitors[0], True, False)

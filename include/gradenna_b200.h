@@ -332,6 +332,40 @@ int gdn_poynting_box_2d_grad(int32_t nx, int32_t ny, int32_t n_freq, const int32
                              const void* dft_hx, const void* dft_hy, const double* g_out,
                              void* g_ez, void* g_hx, void* g_hy, void* stream);
 
+/* The built-in 2D objective L = w_prad sum_k P_k + w_s11 sum_k |S11_k|^2,
+ * P_k the Poynting flux through the dual-grid contour `box` (as
+ * gdn_poynting_box_2d) and S11_k = (V - R I)/(V + R I) of the port at Ez cell
+ * `port`, with V and I rebuilt from the field phasors (freq_adjoint.py:536-558;
+ * monitors.py:20-70; sparams.py:68-79). It reads the forward run's DFT
+ * monitor outputs directly (complex128; any monitor set that covers the
+ * contour's Ez strips, Hx/Hy lines and the port's Ez, Hx, Hy cells) and, in
+ * one launch, writes the value, P_k, S11_k and the adjoint run's CW source
+ * weights: W = conj(dL/dphasor) times the Jz basis -1/cb0 (cb0 = (dt/eps0)/
+ * (dx dy)) on the Ez cells and the magnetic basis Q_MAG/(-dt/mu0) on the Hx
+ * and Hy cells (freq_adjoint.py:317-352), one row of n_freq complex128 per
+ * cell of the lists gdn_tm_objective_cells returns. This replaces scattering
+ * the phasors onto full grids and differentiating the objective with torch. */
+typedef struct GdnTmObjective {
+  int32_t n_freq;
+  int32_t box[4];                    /* il, ir, jb, jt                          */
+  int32_t port[2];                   /* Ez cell (i, j) of the S11 port          */
+  int32_t nx, ny;
+  int32_t n_monitors;
+  const GdnDftMonitor* monitors;     /* host list; out = DEVICE complex128     */
+  const double* freqs;               /* host, n_freq                            */
+  double dx, dy, dt, dz, resistance, w_prad, w_s11, eps0, mu0;
+  double* value;                     /* DEVICE, 1                               */
+  double* p_rad;                     /* DEVICE, n_freq (may be NULL)            */
+  void* s11;                         /* DEVICE complex128 n_freq (may be NULL)  */
+  void *w_ez, *w_hx, *w_hy;          /* DEVICE complex128 (cells, n_freq)       */
+} GdnTmObjective;
+
+/* The objective's cell lists (host int32 (i, j) pairs), in the row order of
+ * w_ez / w_hx / w_hy. Call with NULL lists to get the counts. */
+int gdn_tm_objective_cells(const GdnTmObjective* o, int32_t* n_ez, int32_t* n_hx, int32_t* n_hy,
+                           int32_t* ez_ij, int32_t* hx_ij, int32_t* hy_ij);
+int gdn_tm_objective_prad_s11(const GdnTmObjective* o, void* stream);
+
 /* Design-cell gradient of the frequency-domain adjoint (replaces the numpy
  * contraction of freq_adjoint_gradient, src/gradenna/freq_adjoint.py:454-493):
  *   dL/dtheta = s * sum_k k_norm Re[conj(lam_k) conj(G_k)],

@@ -48,20 +48,20 @@ def test_struct_layouts_match_ctypes(tmp_path):
     src = tmp_path / "sz.cpp"
     src.write_text(
         '#include "gradenna_b200.h"\n#include <cstdio>\n'
-        "int main(){printf(\"%zu %zu %zu %zu %zu %zu %zu\\n\", sizeof(GdnTmParams),"
+        "int main(){printf(\"%zu %zu %zu %zu %zu %zu %zu %zu\\n\", sizeof(GdnTmParams),"
         " sizeof(GdnTmBuffers), sizeof(GdnTmPoints), sizeof(GdnYeeParams), sizeof(GdnYeePoints),"
-        " sizeof(GdnYeeBuffers), sizeof(GdnDftMonitor));}\n")
+        " sizeof(GdnYeeBuffers), sizeof(GdnDftMonitor), sizeof(GdnTmObjective));}\n")
     exe = tmp_path / "sz"
     subprocess.run(["g++", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)],
                    check=True)
     sizes = [int(v) for v in subprocess.run([str(exe)], capture_output=True, text=True,
                                             check=True).stdout.split()]
-    from gradenna_b200 import fdtd3d
+    from gradenna_b200 import fdtd3d, objectives
 
     assert sizes == [ctypes.sizeof(_native.TmParams), ctypes.sizeof(_native.TmBuffers),
                      ctypes.sizeof(_native.TmPoints), ctypes.sizeof(fdtd3d.YeeParams),
                      ctypes.sizeof(fdtd3d.YeePoints), ctypes.sizeof(fdtd3d.YeeBuffers),
-                     ctypes.sizeof(_native.DftMonitor)]
+                     ctypes.sizeof(_native.DftMonitor), ctypes.sizeof(objectives.TmObjective)]
 
 
 def test_bad_arguments_return_status_not_abort():
