@@ -39,6 +39,13 @@ struct Pt3 {
   int m, i, j, k;
 };
 
+// A source point applied by the injection kernels: channel (0 Jz, 1 Jx,
+// 2 Jy, 3 Mx, 4 My, 5 Mz), index in its channel, cell offset in its field.
+struct Fp {
+  int type, m;
+  long long off;
+};
+
 constexpr int MAXF = 64;  // monitors whose offsets the fold stages in shared memory
 
 struct Mon3 {
@@ -63,6 +70,10 @@ struct Dev3 {
   int port_cta;
   const int* off[7];  // per point type CSR over CTAs: src jx jy mx my mz probe
   const Pt3* pts[7];
+  // Source points outside the boxes that hold probes or the port, applied by
+  // yee_inject after the half step (side 0 = E sources, 1 = H sources).
+  const Fp* fpts[2];
+  long long n_fp[2];
   const T *cb_src, *cb_jx, *cb_jy;
   const T* cur[6];  // src jx jy mx my mz
   const T* port_vs;
@@ -144,6 +155,39 @@ __global__ void __launch_bounds__(256) yee_cw_synth(Dev3<T> d, int cnt) {
       }
     d.cwv[(long long)t * d.cw_total + mg] = T(d.cw_env[n0 + t] * s);
   }
+}
+
+// Source injection after a half step (fdtd3d.py:585-588 for Mx/My/Mz,
+// 606-622 for Jx/Jy/Jz): one thread per source point that no step-kernel
+// CTA handles, E = E - c_b,src J or H = H - (dt/mu) M. The step kernels
+// keep only the points of boxes that also hold probes or the port, which
+// must see the source before they read the field; everything else would
+// put a barrier and a point loop into most plane boxes (the adjoint run
+// drives every NTFF face cell).
+template <typename T>
+__global__ void __launch_bounds__(256) yee_inject(Dev3<T> d, int sub, int side) {
+  const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (r >= d.n_fp[side]) return;
+  const Fp p = d.fpts[side][r];
+  const int n = *d.step_base + sub;
+  const int counts[6] = {d.n_src, d.n_jx, d.n_jy, d.n_mx, d.n_my, d.n_mz};
+  const T v = wave(d, p.type, counts[p.type], p.m, n, sub);
+  T coef;
+  int comp;
+  if (p.type == 0) {
+    coef = d.cb_src[p.m];
+    comp = 2;
+  } else if (p.type == 1) {
+    coef = d.cb_jx[p.m];
+    comp = 0;
+  } else if (p.type == 2) {
+    coef = d.cb_jy[p.m];
+    comp = 1;
+  } else {
+    coef = d.dt_mu;
+    comp = p.type;  // 3 hx, 4 hy, 5 hz
+  }
+  atomicAdd(d.f[comp] + p.off, -(coef * v));
 }
 
 // Monitor ring writes of step n (fdtd3d.py:635-662, the running DFT's
@@ -634,8 +678,8 @@ static void comp_shape(int c, int nx, int ny, int nz, int s[3]) {
 struct Layout3 {
   int sy = 0, sz = 0, gj = 0, gk = 0, n_cta = 0, R = 32;
   long long vol = 0, mon_cells = 0;
-  size_t fields, psi, zero_end, off[7], pts[7], pcomp, mons, gsrc, mring, step, eacc, cwv, cls,
-      total;
+  size_t fields, psi, zero_end, off[7], pts[7], pcomp, fpts, mons, gsrc, mring, step, eacc, cwv,
+      cls, total;
 };
 
 // Monitor boxes {comp, lo0, lo1, lo2, s0, s1, s2} in ring order: the listed
@@ -709,6 +753,11 @@ static Layout3 make_layout3(const GdnYeeParams* p, const GdnYeePoints* pts, size
     L.pts[t] = cv.take<Pt3>(std::max(count_of(p, t), 1));
   }
   L.pcomp = cv.take<int>(std::max(p->n_probes, 1));
+  {
+    long long nsrc = 0;
+    for (int t = 0; t < 6; ++t) nsrc += count_of(p, t);
+    L.fpts = cv.take<Fp>(size_t(std::max<long long>(nsrc, 1)));
+  }
   L.mons = cv.take<Mon3>(std::max(p->n_monitors, 6));
   L.gsrc = cv.take<long long>(std::max<size_t>(size_t(L.mon_cells), 1));
   L.mring = cv.take<char>(std::max<size_t>(size_t(L.mon_cells) * L.R, 1) * esize);
@@ -921,19 +970,35 @@ static int run3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuff
     if (p->cw_sources) d.cw_total += count_of(p, t);
   }
 
-  // Point bins by CTA box (i, j/BJ, k/BK).
+  // Point bins by CTA box (i, j/BJ, k/BK). E sources stay in the step
+  // kernel only in boxes that hold probes or the port; every other source
+  // point goes to the injection lists.
+  auto box_of = [&](int i, int j, int k) { return (i * L.gj + j / BJ) * L.gk + k / BK; };
+  std::vector<unsigned char> keep_box(L.n_cta, 0);
+  for (int m = 0; m < p->n_probes; ++m)
+    keep_box[box_of(pts->probe[3 * m], pts->probe[3 * m + 1], pts->probe[3 * m + 2])] = 1;
+  if (p->has_port) keep_box[d.port_cta] = 1;
+  auto in_kernel = [&](int t, int c) { return t == 6 || (t <= 2 && keep_box[c]); };
+  std::vector<Fp> free_pts[2];
   for (int t = 0; t < 7; ++t) {
     const int n = count_of(p, t);
     const int32_t* a = pts_of(pts, t);
     std::vector<int> off(L.n_cta + 1, 0), cta(n);
     for (int m = 0; m < n; ++m) {
-      cta[m] = (a[3 * m] * L.gj + a[3 * m + 1] / BJ) * L.gk + a[3 * m + 2] / BK;
-      off[cta[m] + 1]++;
+      cta[m] = box_of(a[3 * m], a[3 * m + 1], a[3 * m + 2]);
+      if (in_kernel(t, cta[m])) {
+        off[cta[m] + 1]++;
+      } else {
+        const long long cell =
+            ((long long)(a[3 * m] + 1) * L.sy + (a[3 * m + 1] + 1)) * L.sz + (a[3 * m + 2] + 1);
+        free_pts[t >= 3].push_back(Fp{t, m, cell});
+      }
     }
     for (int c = 0; c < L.n_cta; ++c) off[c + 1] += off[c];
     std::vector<Pt3> rec(std::max(n, 1));
     std::vector<int> cur(off.begin(), off.end() - 1);
-    for (int m = 0; m < n; ++m) rec[cur[cta[m]]++] = Pt3{m, a[3 * m], a[3 * m + 1], a[3 * m + 2]};
+    for (int m = 0; m < n; ++m)
+      if (in_kernel(t, cta[m])) rec[cur[cta[m]]++] = Pt3{m, a[3 * m], a[3 * m + 1], a[3 * m + 2]};
     GDN_TRY_CUDA(cudaMemcpyAsync(ws + L.off[t], off.data(), off.size() * sizeof(int),
                                  cudaMemcpyHostToDevice, stream));
     if (n > 0)
@@ -941,6 +1006,17 @@ static int run3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuff
                                    cudaMemcpyHostToDevice, stream));
     d.off[t] = reinterpret_cast<const int*>(ws + L.off[t]);
     d.pts[t] = reinterpret_cast<const Pt3*>(ws + L.pts[t]);
+  }
+  {
+    Fp* base = reinterpret_cast<Fp*>(ws + L.fpts);
+    for (int side = 0; side < 2; ++side) {
+      const size_t nf = free_pts[side].size();
+      d.fpts[side] = base + (side ? free_pts[0].size() : 0);
+      d.n_fp[side] = (long long)nf;
+      if (nf)
+        GDN_TRY_CUDA(cudaMemcpyAsync(const_cast<Fp*>(d.fpts[side]), free_pts[side].data(),
+                                     nf * sizeof(Fp), cudaMemcpyHostToDevice, stream));
+    }
   }
 
   // Monitors.
@@ -1012,9 +1088,10 @@ static int run3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuff
     for (int t = 0; t < 7; ++t) {
       const int n = count_of(p, t);
       const int32_t* a = pts_of(pts, t);
-      for (int m = 0; m < n; ++m)
-        cls[(a[3 * m] * L.gj + a[3 * m + 1] / BJ) * L.gk + a[3 * m + 2] / BK] |=
-            (t >= 3 && t <= 5) ? F_HPTS : F_EPTS;
+      for (int m = 0; m < n; ++m) {
+        const int c = box_of(a[3 * m], a[3 * m + 1], a[3 * m + 2]);
+        if (in_kernel(t, c)) cls[c] |= (t >= 3 && t <= 5) ? F_HPTS : F_EPTS;
+      }
     }
     if (p->has_port) cls[d.port_cta] |= F_EPTS;
     const int m = p->npml;
@@ -1075,12 +1152,20 @@ static int run3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuff
     for (int t = 0; t < cnt; ++t) {
       yee_h<T><<<grd_h, blk, 0, s>>>(d, t, ni_h);
       k += 1;
+      if (d.n_fp[1] > 0) {
+        yee_inject<T><<<unsigned(div_up(d.n_fp[1], 256)), 256, 0, s>>>(d, t, 1);
+        ++k;
+      }
       if (gb1 > 0) {
         yee_gather<T><<<gb1, 256, 0, s>>>(d, t, 1);
         ++k;
       }
       yee_e<T><<<grd_e, blk, 0, s>>>(d, t, ni_e);
       k += 1;
+      if (d.n_fp[0] > 0) {
+        yee_inject<T><<<unsigned(div_up(d.n_fp[0], 256)), 256, 0, s>>>(d, t, 0);
+        ++k;
+      }
       if (gb0 > 0) {
         yee_gather<T><<<gb0, 256, 0, s>>>(d, t, 0);
         ++k;
