@@ -292,7 +292,19 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 5 : 3) yee_h(Dev3<T> d, i
   for (int i = i0; i < i1; ++i, c += di) {
     const int cta = (i * d.gj + blockIdx.y) * d.gk + blockIdx.x;
     const unsigned fl = d.cls[cta];
-    if (live) {
+    if (live && !(fl & F_CPML)) {
+      // No slab within reach of this plane box: the bare update.
+      const T ex0 = ex[c];
+      const T eyk = ey[c + 1], ezj = ez[c + dj], ezi = ez[c + di];
+      const T exk = ex[c + 1], exj = ex[c + dj], eyi = ey[c + di];
+      const T hx0 = hx[c], hy0 = hy[c], hz0 = hz[c];
+      const bool vy = i < nx - 1 && kin, vz = i < nx - 1 && jin;
+      if (vx) hx[c] = hx0 + dt_mu * ((eyk - ey0) * idz - (ezj - ez0) * idy);
+      if (vy) hy[c] = hy0 + dt_mu * ((ezi - ez0) * idx - (exk - ex0) * idz);
+      if (vz) hz[c] = hz0 + dt_mu * ((exj - ex0) * idy - (eyi - ey0) * idx);
+      ey0 = eyi;
+      ez0 = ezi;
+    } else if (live) {
       Ax<T> ax;
       ax.on = slab_coef<T, false>(d, 0, i, nx - 1, ax.b, ax.c, ax.ik);
       // Every operand first (all in the padded volumes), then the updates.
@@ -405,7 +417,29 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 5 : 3) yee_e(Dev3<T> d, i
     const int cta = (i * d.gj + blockIdx.y) * d.gk + blockIdx.x;
     const unsigned fl = d.cls[cta];
     const bool port_here = d.has_port && cta == d.port_cta;
-    if (live) {
+    if (live && !(fl & F_CPML)) {
+      // No slab within reach of this plane box: the bare update.
+      const T hx0 = hx[c], hy0 = hy[c], hz0 = hz[c];
+      const T hzj = hz[c - dj], hyk = hy[c - 1], hxk = hx[c - 1], hxj = hx[c - dj];
+      const T ex0 = ex[c], ey0 = ey[c], ez0 = ez[c];
+      const T ca = d.ca[g], cb = d.cb[g];
+      const bool iin = i >= 1 && i <= nx - 2;
+      const bool vx = i < nx - 1 && vx_jk, vy = iin && vy_jk, vz = iin && vz_jk;
+      if (vx) ex[c] = ca * ex0 + cb * ((hz0 - hzj) * idy - (hy0 - hyk) * idz);
+      if (vy) ey[c] = ca * ey0 + cb * ((hx0 - hxk) * idz - (hz0 - hzi) * idx);
+      if (vz) {
+        const T curl = (hy0 - hyi) * idx - (hx0 - hxj) * idy;
+        const T upd = ca * ez0 + cb * curl;
+        if (port_here && i == d.pi && j == d.pj && k == d.pk) {
+          s_port[0] = ez0;
+          s_port[1] = curl;
+          s_port[2] = upd;
+        }
+        ez[c] = upd;
+      }
+      hyi = hy0;
+      hzi = hz0;
+    } else if (live) {
       Ax<T> ax;
       ax.on = slab_coef<T, true>(d, 0, i - 1, nx - 2, ax.b, ax.c, ax.ik);
       const T hx0 = hx[c], hy0 = hy[c], hz0 = hz[c];
