@@ -229,6 +229,7 @@ def population(seed: int, n_problems: int = POP_N, max_steps: int = 0):
     import gradenna_b200 as gb
     from gradenna_b200.materials import sigma_from_density
     from gradenna_b200.monitors import poynting_box_monitors, port_monitors
+    from gradenna_b200.objectives import RadiatedPowerS11
     from gradenna_b200.topopt import seeded_density
 
     rng = np.random.default_rng(1000 + seed)
@@ -260,14 +261,9 @@ def population(seed: int, n_problems: int = POP_N, max_steps: int = 0):
         for pt in ports:
             mons += port_monitors(pt.ij)
 
-        def obj(ph, grid=grid, box=box):
-            from gradenna_b200.monitors import poynting_flux_box_2d
-            from gradenna_b200.sparams import s11_power_wave
-
-            pwr = poynting_flux_box_2d(ph.dft_ez, ph.dft_hx, ph.dft_hy, grid, box)
-            s = s11_power_wave(ph.port_v[:, 0], ph.port_i[:, 0], RS)
-            return pwr.sum() - (s.real**2 + s.imag**2).sum()
-
+        # sum_k P_rad,k - sum_k |S11_k|^2 of the first port, fused on the device
+        obj = RadiatedPowerS11(grid, box, ports[0].ij, freqs, resistance=RS, w_prad=1.0,
+                               w_s11=-1.0)
         specs.append(dict(grid=grid, objective=obj, design_sigma=sig_d,
                           design_region=(slice(d0, d1), slice(d0, d1)), dft_freqs=freqs, env=env,
                           ports=tuple(ports), cpml=gb.CPMLSpec(npml), dtype=torch.float32,
@@ -706,7 +702,7 @@ def run_population(args):
     dev_specs = [dict(sp, design_sigma=torch.as_tensor(sp["design_sigma"], device=dev))
                  for sp in specs]
     t0 = time.perf_counter()
-    best, tune = autotune_tm_batch(_pop_forward_kwargs(dev_specs, dev), probe_steps=64)
+    best, tune = autotune_tm_batch(_pop_forward_kwargs(dev_specs, dev), probe_steps=128)
     t_tune = time.perf_counter() - t0
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
 

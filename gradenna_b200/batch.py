@@ -123,9 +123,12 @@ def _signature(problems):
 def autotune_tm_batch(problems, *, probe_steps: int = 64, repeats: int = 2, device=None,
                       configs=None, use_cache: bool = True):
     """Pick the tile configuration for a batch by timing its first
-    ``probe_steps`` steps with every configuration (CUDA events, best of
-    ``repeats``). Returns (best_config, {config: seconds}); the choice is
-    cached per population signature (grid sizes, frequency and port counts).
+    ``probe_steps`` steps with every configuration: the device time of the
+    time loops alone (CUDA events around the loops, gdn_tm_loop_stats), best
+    of ``repeats``, so the per-call host set-up, which is the same for every
+    configuration and dominates a short probe, does not decide. Returns
+    (best_config, {config: seconds}); the choice is cached per population
+    signature (grid sizes, frequency and port counts).
     """
     key = (_signature(problems), probe_steps)
     if use_cache and key in _TUNE_CACHE:
@@ -137,13 +140,11 @@ def autotune_tm_batch(problems, *, probe_steps: int = 64, repeats: int = 2, devi
         best = None
         simulate_tm_batch(short, tile_config=cfg, device=dev)  # warm-up
         for _ in range(repeats):
-            e0 = torch.cuda.Event(enable_timing=True)
-            e1 = torch.cuda.Event(enable_timing=True)
-            e0.record()
-            simulate_tm_batch(short, tile_config=cfg, device=dev)
-            e1.record()
             torch.cuda.synchronize(dev)
-            t = e0.elapsed_time(e1) / 1e3
+            _native.tm_loop_stats(reset=True)
+            simulate_tm_batch(short, tile_config=cfg, device=dev)
+            torch.cuda.synchronize(dev)
+            t = _native.tm_loop_stats(reset=True)[0] / 1e3
             best = t if best is None else min(best, t)
         timings[cfg] = best
     choice = (min(timings, key=timings.get), timings)
@@ -181,9 +182,8 @@ def freq_adjoint_gradient_batch(specs, *, tile_config: int | None = None, device
                              in zip(plans, designs)], tile_config=tile_config, device=dev)
     adj_kw, adj_at, cots = [], [], []
     for k, ((pl, obj, _, _), (e, s), res) in enumerate(zip(plans, designs, fwd)):
-        full = fa._scatter_full(pl, res)
-        _, cot = fa._cotangents(pl, obj, full, res)
-        kw = fa._adjoint_kwargs(pl, e, s, fa._adjoint_sources(pl, cot))
+        _, srcs = fa._objective_sources(pl, obj, res)
+        kw = fa._adjoint_kwargs(pl, e, s, srcs)
         if kw is not None:
             adj_at.append(k)
             adj_kw.append(kw)
