@@ -22,6 +22,7 @@ CPU fallback.
 from __future__ import annotations
 
 import ctypes
+import functools
 from typing import NamedTuple
 
 import numpy as np
@@ -154,6 +155,42 @@ def phase_tables(freqs, n_steps: int, dt: float, step0: int = 0):
     ph_e = np.exp(-2j * np.pi * np.outer(nn + 1.0, f) * dt)
     ph_h = np.exp(-2j * np.pi * np.outer(nn + 0.5, f) * dt)
     return ph_e, ph_h
+
+
+@functools.lru_cache(maxsize=256)
+def _phase_tables_dev(freqs: tuple, n_steps: int, dt: float, device: torch.device):
+    """phase_tables on the device, cached: the forward and adjoint runs of a
+    problem, and every iteration of an optimisation, read the same tables.
+    The kernels only read them."""
+    ph_e, ph_h = phase_tables(freqs, n_steps, dt)
+    return torch.as_tensor(ph_e, device=device), torch.as_tensor(ph_h, device=device)
+
+
+@functools.lru_cache(maxsize=256)
+def _cpml_tables_dev(nx: int, ny: int, dx: float, dy: float, dt: float, cpml: CPMLSpec,
+                     npdt, device: torch.device):
+    """The 2D CPML slab tables and 1/kappa tables on the device
+    (fdtd2d.py:354-374), cached per grid, CPML and dtype; read-only."""
+    npml = cpml.thickness
+    cx_e = axis_coefficients(nx, dx, dt, cpml, half=False, dtype=npdt)
+    cx_h = axis_coefficients(nx, dx, dt, cpml, half=True, dtype=npdt)
+    cy_e = axis_coefficients(ny, dy, dt, cpml, half=False, dtype=npdt)
+    cy_h = axis_coefficients(ny, dy, dt, cpml, half=True, dtype=npdt)
+    tabs = {}
+    for key, (b, c) in {
+        "ezx": (cx_e.b[1:-1], cx_e.c[1:-1]), "ezy": (cy_e.b[1:-1], cy_e.c[1:-1]),
+        "hyx": (cx_h.b, cx_h.c), "hxy": (cy_h.b, cy_h.c),
+    }.items():
+        b_lo, c_lo, b_hi, c_hi = slab_tables(b, c, npml)
+        for nm, arr in (("b_lo", b_lo), ("c_lo", c_lo), ("b_hi", b_hi), ("c_hi", c_hi)):
+            tabs[f"{nm[0]}_{key}_{nm[2:]}"] = torch.as_tensor(
+                np.ascontiguousarray(arr) if arr.size else np.zeros(1, npdt), device=device)
+    ik = {
+        "inv_kx_e": cx_e.inv_kappa[1:-1], "inv_ky_e": cy_e.inv_kappa[1:-1],
+        "inv_kx_h": cx_h.inv_kappa, "inv_ky_h": cy_h.inv_kappa,
+    }
+    ik = {k: torch.as_tensor(np.ascontiguousarray(v), device=device) for k, v in ik.items()}
+    return tabs, ik
 
 
 def _i32(a) -> ctypes.POINTER(ctypes.c_int32):
@@ -296,26 +333,10 @@ def _prepare_tm(
     else:
         cb_vs = torch.zeros(0, dtype=fdt, device=dev)
 
-    # CPML tables (fdtd2d.py:354-374).
+    # CPML tables (fdtd2d.py:354-374), built once per grid, CPML and dtype.
     npml = cpml.thickness
-    cx_e = axis_coefficients(nx, grid.dx, dt, cpml, half=False, dtype=npdt)
-    cx_h = axis_coefficients(nx, grid.dx, dt, cpml, half=True, dtype=npdt)
-    cy_e = axis_coefficients(ny, grid.dy, dt, cpml, half=False, dtype=npdt)
-    cy_h = axis_coefficients(ny, grid.dy, dt, cpml, half=True, dtype=npdt)
-    tabs = {}
-    for key, (b, c) in {
-        "ezx": (cx_e.b[1:-1], cx_e.c[1:-1]), "ezy": (cy_e.b[1:-1], cy_e.c[1:-1]),
-        "hyx": (cx_h.b, cx_h.c), "hxy": (cy_h.b, cy_h.c),
-    }.items():
-        b_lo, c_lo, b_hi, c_hi = slab_tables(b, c, npml)
-        for nm, arr in (("b_lo", b_lo), ("c_lo", c_lo), ("b_hi", b_hi), ("c_hi", c_hi)):
-            tabs[f"{nm[0]}_{key}_{nm[2:]}"] = torch.as_tensor(
-                np.ascontiguousarray(arr) if arr.size else np.zeros(1, npdt), device=dev)
-    ik = {
-        "inv_kx_e": cx_e.inv_kappa[1:-1], "inv_ky_e": cy_e.inv_kappa[1:-1],
-        "inv_kx_h": cx_h.inv_kappa, "inv_ky_h": cy_h.inv_kappa,
-    }
-    ik = {k: torch.as_tensor(np.ascontiguousarray(v), device=dev) for k, v in ik.items()}
+    tabs, ik = _cpml_tables_dev(nx, ny, float(grid.dx), float(grid.dy), float(dt), cpml, npdt,
+                                torch.device(dev))
 
     # DFT (fdtd2d.py:384-398).
     dft_freqs = tuple(float(f) for f in dft_freqs)
@@ -329,9 +350,7 @@ def _prepare_tm(
             raise ValueError(f"dft_dtype must be a complex dtype, got {dft_dtype}")
     ph_e_t = ph_h_t = None
     if n_freq:
-        ph_e, ph_h = phase_tables(dft_freqs, n_steps, dt)
-        ph_e_t = torch.as_tensor(ph_e, device=dev)
-        ph_h_t = torch.as_tensor(ph_h, device=dev)
+        ph_e_t, ph_h_t = _phase_tables_dev(dft_freqs, int(n_steps), float(dt), torch.device(dev))
     if cw_sources is not None and not n_freq:
         raise ValueError("cw_sources needs dft_freqs")
 

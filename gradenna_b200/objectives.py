@@ -64,6 +64,7 @@ class RadiatedPowerS11:
         self.resistance = float(resistance)
         self.w_prad = float(w_prad)
         self.w_s11 = float(w_s11)
+        self._cells = None
 
     def monitors(self):
         return poynting_box_monitors(self.box) + port_monitors(self.port_ij)
@@ -99,7 +100,10 @@ class RadiatedPowerS11:
         return d, (arr, fr)
 
     def cells(self):
-        """Host (n, 2) int32 cell lists (Ez, Hx, Hy) of the adjoint weights' rows."""
+        """Host (n, 2) int32 cell lists (Ez, Hx, Hy) of the adjoint weights' rows
+        (computed once per objective: they depend on the geometry only)."""
+        if self._cells is not None:
+            return [c.copy() for c in self._cells]
         lib = _native.load()
         d, keep = self._desc(self.freqs, [], [])
         n = [ctypes.c_int32() for _ in range(3)]
@@ -109,7 +113,8 @@ class RadiatedPowerS11:
         _native.check(lib.gdn_tm_objective_cells(
             ctypes.byref(d), None, None, None,
             *(a.ctypes.data_as(_native.P_i32) for a in lists)))
-        return lists
+        self._cells = lists
+        return [c.copy() for c in lists]
 
     def fused_tm(self, mons, outs, device):
         """(value, p_rad, s11, [(ez_idx, W), (hx_idx, W), (hy_idx, W)]) from the
