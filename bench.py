@@ -367,15 +367,16 @@ class ClockSampler:
          "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
          "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
-    def __init__(self, index: int):
+    def __init__(self, index: int, interval_ms: int = 200):
         self.index = index
+        self.interval_ms = int(interval_ms)
         self.proc = None
 
     def __enter__(self):
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
-                 "--format=csv,noheader,nounits", "-lms", "200"],
+                 "--format=csv,noheader,nounits", "-lms", str(self.interval_ms)],
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
         except OSError:
             self.proc = None
@@ -722,7 +723,9 @@ def run_population(args):
     barrier()
     l0 = _native.kernel_launches()
     _native.tm_loop_stats(reset=True)
-    with ClockSampler(local) as clk:
+    # The population's step is host-bound (tens of thousands of launches); a
+    # 5 Hz nvidia-smi poll measurably slows it, so clocks are sampled at 1 Hz.
+    with ClockSampler(local, interval_ms=1000) as clk:
         for _ in range(args.steps):
             flush.fill_(1.0)
             e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
