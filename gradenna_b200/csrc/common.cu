@@ -97,7 +97,16 @@ cudaStream_t capture_stream() {
   cudaGetDevice(&dev);
   std::lock_guard<std::mutex> lock(mu);
   if (dev < 0 || dev >= 64) return nullptr;
-  if (!streams[dev]) cudaStreamCreateWithFlags(&streams[dev], cudaStreamNonBlocking);
+  if (!streams[dev]) {
+    // Highest priority: captured kernel nodes keep it (graphs instantiated
+    // with cudaGraphInstantiateFlagUseNodePriority), so the 2D general
+    // tiles, which have fewer and longer CTAs, are dispatched before the
+    // interior tiles captured on the side stream (measured: the 4-step
+    // block 34.2 -> 33.1 us at 1024^2).
+    int lo = 0, hi = 0;
+    cudaDeviceGetStreamPriorityRange(&lo, &hi);
+    cudaStreamCreateWithPriority(&streams[dev], cudaStreamNonBlocking, hi);
+  }
   return streams[dev];
 }
 

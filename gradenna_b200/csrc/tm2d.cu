@@ -1653,7 +1653,7 @@ static int run(const GdnTmParams* p, const GdnTmPoints* pts, const GdnTmBuffers*
       set_error("graph capture failed: %s", cudaGetErrorString(e1));
       return GDN_ERR_CUDA;
     }
-    const cudaError_t e2 = cudaGraphInstantiate(exec, g, 0);
+    const cudaError_t e2 = cudaGraphInstantiate(exec, g, cudaGraphInstantiateFlagUseNodePriority);
     cudaGraphDestroy(g);
     if (e2 != cudaSuccess) {
       set_error("graph instantiate failed: %s", cudaGetErrorString(e2));
