@@ -1175,8 +1175,29 @@ static int run3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuff
   const dim3 grd_h(L.gk, L.gj, unsigned(div_up(nx, ni_h)));
   const dim3 grd_e(L.gk, L.gj, unsigned(div_up(nx, ni_e)));
   const int eblocks = int(std::min<long long>(div_up((long long)nx * ny * nz, 256), 148 * 8));
-  auto enqueue = [&](int cnt, cudaStream_t s) -> uint64_t {
+  // Chunk body. With a side stream the ring gathers run beside the step
+  // kernels: a gather only reads the field it copies, so the H gather of
+  // step t overlaps yee_e of step t and the E gather overlaps yee_h of step
+  // t + 1; each field's next writer waits for its gather (events), and the
+  // fold waits for the last ones.
+  auto enqueue = [&](int cnt, cudaStream_t s, cudaStream_t side, cudaEvent_t* ev) -> uint64_t {
     uint64_t k = 0;
+    bool pend_h = false, pend_e = false;  // a gather still reads H / E
+    auto gather = [&](int t, int sd, unsigned blocks) {
+      if (!side) {
+        yee_gather<T><<<blocks, 256, 0, s>>>(d, t, sd);
+        return;
+      }
+      cudaEventRecord(ev[sd], s);
+      cudaStreamWaitEvent(side, ev[sd], 0);
+      yee_gather<T><<<blocks, 256, 0, side>>>(d, t, sd);
+      cudaEventRecord(ev[2 + sd], side);
+      (sd ? pend_h : pend_e) = true;
+    };
+    auto settle = [&](bool& pend, int sd) {  // the field's gather has finished
+      if (pend) cudaStreamWaitEvent(s, ev[2 + sd], 0);
+      pend = false;
+    };
     if (d.cw_total > 0) {
       yee_cw_synth<T><<<unsigned(div_up(d.cw_total, 256)), 256,
                         2 * size_t(cnt) * p->n_freq * sizeof(double2), s>>>(d, cnt);
@@ -1184,6 +1205,7 @@ static int run3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuff
     }
     const unsigned gb0 = unsigned(div_up(d.gcells[0], 256)), gb1 = unsigned(div_up(d.gcells[1], 256));
     for (int t = 0; t < cnt; ++t) {
+      settle(pend_h, 1);
       yee_h<T><<<grd_h, blk, 0, s>>>(d, t, ni_h);
       k += 1;
       if (d.n_fp[1] > 0) {
@@ -1191,9 +1213,10 @@ static int run3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuff
         ++k;
       }
       if (gb1 > 0) {
-        yee_gather<T><<<gb1, 256, 0, s>>>(d, t, 1);
+        gather(t, 1, gb1);
         ++k;
       }
+      settle(pend_e, 0);
       yee_e<T><<<grd_e, blk, 0, s>>>(d, t, ni_e);
       k += 1;
       if (d.n_fp[0] > 0) {
@@ -1201,7 +1224,7 @@ static int run3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuff
         ++k;
       }
       if (gb0 > 0) {
-        yee_gather<T><<<gb0, 256, 0, s>>>(d, t, 0);
+        gather(t, 0, gb0);
         ++k;
       }
       if (p->record_energy) {
@@ -1209,6 +1232,8 @@ static int run3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuff
         ++k;
       }
     }
+    settle(pend_h, 1);
+    settle(pend_e, 0);
     if (!mons.empty()) {
       if (f64acc)
         launch_fold3<T, double>(d, mons, max_cells, cnt, p->n_freq, s);
@@ -1222,8 +1247,20 @@ static int run3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuff
   auto capture = [&](int cnt, cudaGraphExec_t* exec, uint64_t* nodes) -> int {
     cudaStream_t cs = capture_stream();
     if (!cs) GDN_BAD_ARG("no capture stream for this device");
+    cudaStream_t side = capture_side_stream();
+    cudaEvent_t ev[4] = {};
+    bool evs = side != nullptr;
+    for (int e = 0; e < 4 && evs; ++e)
+      evs = cudaEventCreateWithFlags(&ev[e], cudaEventDisableTiming) == cudaSuccess;
+    struct EvGuard {
+      cudaEvent_t* e;
+      ~EvGuard() {
+        for (int q = 0; q < 4; ++q)
+          if (e[q]) cudaEventDestroy(e[q]);
+      }
+    } ev_guard{ev};
     GDN_TRY_CUDA(cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal));
-    *nodes = enqueue(cnt, cs);
+    *nodes = enqueue(cnt, cs, evs ? side : nullptr, ev);
     cudaGraph_t g = nullptr;
     const cudaError_t e1 = cudaStreamEndCapture(cs, &g);
     if (e1 != cudaSuccess) {
