@@ -157,6 +157,17 @@ __global__ void __launch_bounds__(256) yee_cw_synth(Dev3<T> d, int cnt) {
   }
 }
 
+// Programmatic dependent launch: the step and injection kernels of a chunk
+// are launched with programmatic stream serialisation, so the next kernel's
+// CTAs are scheduled as this kernel's CTAs drain instead of after a full
+// launch round trip. Every such kernel first waits until its predecessor
+// grid has completed and its writes are visible (griddepcontrol.wait, a
+// no-op for a normal launch), then allows its own dependents to launch.
+__device__ __forceinline__ void dependent_launch_gate() {
+  asm volatile("griddepcontrol.wait;\n" ::: "memory");
+  asm volatile("griddepcontrol.launch_dependents;\n" ::: "memory");
+}
+
 // Source injection after a half step (fdtd3d.py:585-588 for Mx/My/Mz,
 // 606-622 for Jx/Jy/Jz): one thread per source point that no step-kernel
 // CTA handles, E = E - c_b,src J or H = H - (dt/mu) M. The step kernels
@@ -166,6 +177,7 @@ __global__ void __launch_bounds__(256) yee_cw_synth(Dev3<T> d, int cnt) {
 // drives every NTFF face cell).
 template <typename T>
 __global__ void __launch_bounds__(256) yee_inject(Dev3<T> d, int sub, int side) {
+  dependent_launch_gate();
   const long long r = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (r >= d.n_fp[side]) return;
   const Fp p = d.fpts[side][r];
@@ -261,6 +273,7 @@ __device__ __forceinline__ T psi_term(const Ax<T>& a, T diff, T& psi) {
 // ---------------------------------------------------------------------------
 template <typename T>
 __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 5 : 3) yee_h(Dev3<T> d, int sub, int ni) {
+  dependent_launch_gate();
   const int n = *d.step_base + sub;
   const int k = blockIdx.x * BK + threadIdx.x;
   const int j = blockIdx.y * BJ + threadIdx.y;
@@ -383,6 +396,7 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 5 : 3) yee_h(Dev3<T> d, i
 template <typename T>
 __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 5 : 3) yee_e(Dev3<T> d, int sub, int ni) {
   __shared__ T s_port[3];  // Ez^n, curl_z and the plain-updated Ez at the port edge
+  dependent_launch_gate();
   const int n = *d.step_base + sub;
   const int k = blockIdx.x * BK + threadIdx.x;
   const int j = blockIdx.y * BJ + threadIdx.y;
@@ -886,6 +900,23 @@ static int validate3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYe
   return GDN_OK;
 }
 
+// Launch with programmatic stream serialisation (see dependent_launch_gate).
+template <typename... KArgs, typename... Args>
+static void launch_pdl(void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t s,
+                       Args... args) {
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = grid;
+  cfg.blockDim = block;
+  cfg.dynamicSmemBytes = 0;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+  at[0].val.programmaticStreamSerializationAllowed = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  cudaLaunchKernelEx(&cfg, kernel, args...);
+}
+
 // Planes per CTA for a step kernel: the CTAs of `cols` (j, k) tile columns
 // split the nx planes so that the whole grid is one wave of resident CTAs.
 template <typename K>
@@ -1206,10 +1237,10 @@ static int run3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuff
     const unsigned gb0 = unsigned(div_up(d.gcells[0], 256)), gb1 = unsigned(div_up(d.gcells[1], 256));
     for (int t = 0; t < cnt; ++t) {
       settle(pend_h, 1);
-      yee_h<T><<<grd_h, blk, 0, s>>>(d, t, ni_h);
+      launch_pdl(yee_h<T>, grd_h, blk, s, d, t, ni_h);
       k += 1;
       if (d.n_fp[1] > 0) {
-        yee_inject<T><<<unsigned(div_up(d.n_fp[1], 256)), 256, 0, s>>>(d, t, 1);
+        launch_pdl(yee_inject<T>, dim3(unsigned(div_up(d.n_fp[1], 256))), dim3(256), s, d, t, 1);
         ++k;
       }
       if (gb1 > 0) {
@@ -1217,10 +1248,10 @@ static int run3(const GdnYeeParams* p, const GdnYeePoints* pts, const GdnYeeBuff
         ++k;
       }
       settle(pend_e, 0);
-      yee_e<T><<<grd_e, blk, 0, s>>>(d, t, ni_e);
+      launch_pdl(yee_e<T>, grd_e, blk, s, d, t, ni_e);
       k += 1;
       if (d.n_fp[0] > 0) {
-        yee_inject<T><<<unsigned(div_up(d.n_fp[0], 256)), 256, 0, s>>>(d, t, 0);
+        launch_pdl(yee_inject<T>, dim3(unsigned(div_up(d.n_fp[0], 256))), dim3(256), s, d, t, 0);
         ++k;
       }
       if (gb0 > 0) {
