@@ -427,9 +427,10 @@ def profiled_traffic(name):
     (its traffic_bytes_per_launch line), or None."""
     path = os.path.join(ROOT, "profiles", name)
     try:
-        for line in open(path):
-            if line.startswith("traffic_bytes_per_launch:"):
-                return int(float(line.split(":", 1)[1].split()[0]))
+        with open(path) as f:
+            for line in f:
+                if line.startswith("traffic_bytes_per_launch:"):
+                    return int(float(line.split(":", 1)[1].split()[0]))
     except OSError:
         pass
     return None
